@@ -1,0 +1,270 @@
+/* libmvs_b200 -- C ABI of the B200 (sm_100a) multiview-stereo kernels.
+ *
+ * Plain C: POD structs, raw pointers, sizes and an opaque stream handle
+ * (a cudaStream_t passed as void*; NULL is the legacy default stream).  Every
+ * call returns an int status (MVS_OK == 0, negative on failure); the message
+ * of the last failure on the calling thread is mvs_last_error().  No call
+ * resets the device.
+ *
+ * Pointer naming: d_* are device pointers, h_* host pointers.  Images are
+ * dense row-major float32, stride == width, as the reference forces for every
+ * image it allocates (memory.h:113-122).
+ *
+ * Each entry point names the reference interface it replaces.  The reference
+ * exposes no C or FFI surface of its own: its callers are the C++ class
+ * PlaneSweep (planesweep.h:27-510) and the free kernel wrappers of
+ * kernels.cu.h and fusion.cu.h.  The class-level API is mirrored by the
+ * mvs_ps_* and mvs_fusion_* handle functions below and by the C++ classes in
+ * include/mvs_b200.hpp.
+ */
+#ifndef MVS_B200_H
+#define MVS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------ */
+#define MVS_OK 0
+#define MVS_ERR_ARG -1      /* bad argument (null pointer, size, even window ...) */
+#define MVS_ERR_NOMEM -2    /* device or host allocation failed */
+#define MVS_ERR_CUDA -3     /* a CUDA runtime call or launch failed */
+#define MVS_ERR_TIMEOUT -4  /* a bounded device-side wait gave up */
+#define MVS_ERR_STATE -5    /* call out of order (e.g. denoise before a sweep) */
+#define MVS_ERR_NOTBUILT -6 /* library built without the requested variant */
+
+/* Message of the last failing call on this thread ("" after success). */
+const char *mvs_last_error(void);
+/* 10000 * major + 100 * minor + patch. */
+int mvs_version(void);
+/* Select the device for the calling thread (replaces PlaneSweep::cudaDevInit,
+ * planesweep.cpp:30-58, without the device reset of cudaReset()). */
+int mvs_set_device(int device);
+
+/* ---- plane sweep ----------------------------------------------------------
+ * Replaces the per-plane launch chain of PlaneSweep::PlaneSweepThread
+ * (planesweep.cpp:163-259: transform_indexes, bilinear_interpolation,
+ * windowed_mean_row/column, calculate_STD, element_multiply, calcNCC,
+ * update_arrays, kernels.cu:4-235) and the epilogue of
+ * PlaneSweep::RunAlgorithm (sum_depthmap_NCC, element_rdivide,
+ * set_QNAN_value, kernels.cu:84-101,145-157,331-340; planesweep.cpp:105-131)
+ * with fused kernels. */
+
+#define MVS_MOMENTS_REFERENCE 0   /* the reference's naive box means, its order
+                                     of operations and roundings */
+#define MVS_MOMENTS_COMPENSATED 1 /* shifted FP32 window sums: E[x^2]-E[x]^2
+                                     without catastrophic cancellation */
+
+#define MVS_SWEEP_PER_VIEW 0   /* the reference: per-view NCC argmax, then the
+                                  average of per-view depths above the NCC
+                                  threshold (NaN -> zfar) */
+#define MVS_SWEEP_AGGREGATED 1 /* extension: cost = 1 - mean NCC over views,
+                                  stored as a BF16 cost volume [P][H][W],
+                                  winner-take-all argmin per pixel */
+
+typedef struct mvs_sweep_desc {
+    int32_t width, height;  /* all views share the reference's size */
+    int32_t n_views;        /* source views */
+    int32_t n_planes;
+    int32_t window;         /* odd, 3..15 (PlaneSweep::setWindowSize, planesweep.h:234) */
+    int32_t moments;        /* MVS_MOMENTS_* */
+    int32_t mode;           /* MVS_SWEEP_* */
+    float std_threshold;    /* NCC := 0 where either window std is below (kernels.cu:59) */
+    float ncc_threshold;    /* per-view depths with best NCC <= this are not averaged (kernels.cu:96) */
+    float zfar;             /* depth written where no view passes (planesweep.cpp:131) */
+} mvs_sweep_desc;
+
+/* Bytes of device workspace mvs_sweep needs for `desc` when the optional
+ * per-view outputs are not supplied. */
+size_t mvs_sweep_workspace_bytes(const mvs_sweep_desc *desc);
+
+/* Per-plane homographies built in FP64 on the device and stored as float:
+ * H[v][p] = K (Rrel_v + trel_v e3^T / depth_p) K^-1, normalised so H22 = 1
+ * (the matrix PlaneSweepThread builds in float on the host,
+ * planesweep.cpp:195-203).  K is the reference's 1-based calibration matrix
+ * (pixel (l,k) is (l+1,k+1)); Rrel/trel are reference->source
+ * (PlaneSweep::RelativeMatrices).  h_K9: 9 doubles, h_Rrel: n_views*9,
+ * h_trel: n_views*3 (host); d_depths: n_planes floats; d_H: n_views*n_planes*9
+ * floats (device). */
+int mvs_sweep_homographies(const mvs_sweep_desc *desc, const double *h_K9, const double *h_Rrel,
+                           const double *h_trel, const float *d_depths, float *d_H, void *stream);
+
+/* The fused sweep.  d_ref: H*W; d_srcs: n_views*H*W (0..255 grey);
+ * d_H: n_views*n_planes*9 (as above); d_depths: n_planes.
+ * Outputs (device):
+ *   d_depth   H*W, required.  PER_VIEW: the averaged depthmap RunAlgorithm
+ *             copies back.  AGGREGATED: depth of the winning plane.
+ *   d_labels  PER_VIEW: n_views*H*W best plane index per view (-1: no plane
+ *             with NCC > 0); AGGREGATED: H*W winning plane.  May be NULL.
+ *   d_best    PER_VIEW: n_views*H*W best NCC per view (devbestNCC);
+ *             AGGREGATED: H*W winning cost.  May be NULL.
+ *   d_cost    AGGREGATED only: n_planes*H*W BF16 cost volume.  May be NULL.
+ * d_workspace/workspace_bytes: at least mvs_sweep_workspace_bytes(desc) when
+ * d_labels or d_best is NULL (PER_VIEW), else may be NULL. */
+int mvs_sweep(const mvs_sweep_desc *desc, const float *d_ref, const float *d_srcs, const float *d_H,
+              const float *d_depths, float *d_depth, int32_t *d_labels, float *d_best, uint16_t *d_cost,
+              void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* Winner-take-all argmin over a stored BF16 cost volume (d_cost:
+ * n_planes * n_pixels, as mvs_sweep writes it; n_pixels divisible by 8).
+ * Writes the winning plane's depth (zfar if none), optional label and cost. */
+int mvs_sweep_wta_volume(const uint16_t *d_cost, const float *d_depths, int32_t n_pixels, int32_t n_planes,
+                         float zfar, float *d_depth, int32_t *d_labels, float *d_best, void *stream);
+
+/* ---- TGV2 multiview refinement ------------------------------------------
+ * Replaces the launch chain of PlaneSweep::TGV (planesweep.cpp:381-536):
+ * Anisotropic_diffusion_tensor, the per-view linearisation
+ * (TGV2_transform_coordinates, TGV2_calculate_coordinate_derivatives,
+ * TGV2_calculate_derivativeF, bilinear_interpolation, TGV2_calculate_Iu,
+ * subtract) and the iteration (TGV2_updateP_tensor_weighed, TGV2_updateQ,
+ * TGV2_updateR, TGV2_updateU_tensor_weighed), TGV2_kernels.cu:54-365. */
+typedef struct mvs_tgv2_params {
+    int32_t niters;       /* iterations per linearisation (reference: niters) */
+    int32_t warps;        /* linearisations (reference: warps) */
+    double lambda, alpha0, alpha1, tau, sigma, beta, gamma; /* as PlaneSweep::TGV */
+    double tol;           /* extension: stop once |dE| <= tol*|E| between two
+                             checks inside one linearisation; 0 = fixed count */
+    int32_t check_every;  /* iterations between energy evaluations (tol > 0) */
+    int32_t max_iters;    /* extension: total cap (0 = warps * niters) */
+} mvs_tgv2_params;
+
+size_t mvs_tgv2_workspace_bytes(int32_t width, int32_t height, int32_t n_views);
+
+/* d_ref255: H*W, d_srcs255: n_views*H*W (0..255).  h_K9/h_invK9: the
+ * reference's float K (1-based) and K^-1; h_Rrel: n_views*9, h_trel:
+ * n_views*3 (float, as PlaneSweep::RelativeMatrices computes them).
+ * d_u: H*W, in: start depth (NULL-equivalent: pass u_init_const = 1 and the
+ * reference's constant start is used when `u_from_input` is 0); out: result.
+ * iters_out / energy_out (host, may be NULL): iterations run and last
+ * energy (FP64, evaluated on the device). */
+int mvs_tgv2_run(int32_t width, int32_t height, int32_t n_views, const float *d_ref255, const float *d_srcs255,
+                 const float *h_K9, const float *h_invK9, const float *h_Rrel, const float *h_trel,
+                 const mvs_tgv2_params *params, int32_t u_from_input, float u_init_const, float *d_u,
+                 int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
+                 void *stream);
+
+/* ---- TV-L1 depth denoise --------------------------------------------------
+ * Replaces PlaneSweep::CudaDenoise's chain (planesweep.cpp:297-379):
+ * Anisotropic_diffusion_tensor + denoising_TVL1_calculateP_tensor_weighed +
+ * denoising_TVL1_update (kernels.cu:283-370). d_depth: in/out, H*W. */
+typedef struct mvs_tvl1_params {
+    int32_t niters;
+    double lambda, tau, sigma, theta, beta, gamma; /* as PlaneSweep::CudaDenoise */
+} mvs_tvl1_params;
+
+size_t mvs_tvl1_workspace_bytes(int32_t width, int32_t height);
+
+int mvs_tvl1_denoise(int32_t width, int32_t height, const float *d_ref255, float *d_depth, float znear, float zfar,
+                     const mvs_tvl1_params *params, void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* ---- back-projection --------------------------------------------------------
+ * Replaces compute3D (kernels.cu:405-429) as PlaneSweep::get3Dcoordinates
+ * drives it (planesweep.cpp:551-586): for z < 5.5, X = Rr (z K^-1 (x+1,y+1,1)) + t;
+ * else Z = -9 and X, Y are left untouched.  h_* are float 3x3 / 3-vectors. */
+int mvs_compute3d(int32_t width, int32_t height, const float *d_depth, const float *h_invK9, const float *h_Rr9,
+                  const float *h_t3, float *d_X, float *d_Y, float *d_Z, void *stream);
+
+/* ---- TV-L1 histogram fusion -------------------------------------------------
+ * Replaces fusionData<N, Device> (fusion.h:105-1055) and the launch wrappers
+ * FusionUpdateHistogram / FusionUpdateU / FusionUpdateP /
+ * FusionUpdateIteration (fusion.cu:72-99, fusion.cu.h:40-173).
+ *
+ * Layout (SoA, x fastest, n = width*height*depth voxels):
+ *   u[n], v[n] float; p[3][n] float; hist[n][hist_stride] uint16 (bins counts
+ *   per voxel, padded to hist_stride = 8 or 16 for 128-bit access). */
+typedef struct mvs_fusion mvs_fusion;
+
+int mvs_fusion_create(int32_t width, int32_t height, int32_t depth, int32_t bins, const float *corner_a,
+                      const float *corner_b, mvs_fusion **out);
+int mvs_fusion_destroy(mvs_fusion *f);
+int mvs_fusion_set_volume(mvs_fusion *f, const float *corner_a, const float *corner_b);
+/* Zero u, v, p and the histograms. */
+int mvs_fusion_reset(mvs_fusion *f, void *stream);
+/* Histogram votes of n_maps depthmaps (d_depths: n_maps*h*w device floats,
+ * h_K/h_R: n_maps*9 floats, h_t: n_maps*3: world->camera, 0-based K), in map
+ * order, in one voxel pass (fusion.cu:5-43 + fusionData::updateHist). */
+int mvs_fusion_histogram(mvs_fusion *f, const float *d_depths, int32_t n_maps, int32_t w, int32_t h,
+                         const float *h_K, const float *h_R, const float *h_t, float threshold, void *stream);
+/* n_iters TV-L1 primal-dual iterations, each FusionUpdateU then
+ * FusionUpdateP (fusion.cu:45-70), fused into one voxel pass per iteration. */
+int mvs_fusion_tvl1(mvs_fusion *f, int32_t n_iters, double tau, double lambda, double sigma, void *stream);
+/* Single steps at the reference's granularity. */
+int mvs_fusion_update_u(mvs_fusion *f, double tau, double lambda, void *stream);
+int mvs_fusion_update_p(mvs_fusion *f, double sigma, void *stream);
+/* FusionUpdateIteration: one depthmap's histogram votes, then U, then P. */
+int mvs_fusion_iteration(mvs_fusion *f, const float *d_depth, int32_t w, int32_t h, const float *h_K9,
+                         const float *h_R9, const float *h_t3, float threshold, double tau, double lambda,
+                         double sigma, void *stream);
+/* Host copies of the state (NULL skips a field).  h_p: 3*n, h_hist: bins*n
+ * (plane per bin). */
+int mvs_fusion_download(mvs_fusion *f, float *h_u, float *h_v, float *h_p, uint16_t *h_hist);
+int mvs_fusion_upload(mvs_fusion *f, const float *h_u, const float *h_v, const float *h_p, const uint16_t *h_hist);
+/* Device pointers of the current state (valid until the next call on f). */
+int mvs_fusion_device_state(mvs_fusion *f, float **d_u, float **d_v, float **d_p, uint16_t **d_hist,
+                            int32_t *hist_stride);
+/* World coordinates of the voxels with lo < u < hi (the GUI keeps
+ * -1 < u < 0, pclviewer.cpp:1058-1074), x fastest; h_xyz: 3*capacity floats.
+ * *count receives the number of such voxels (may exceed capacity). */
+int mvs_fusion_extract(mvs_fusion *f, float lo, float hi, float *h_xyz, int64_t capacity, int64_t *count);
+
+/* ---- PlaneSweep drop-in handle ------------------------------------------------
+ * Mirrors class PlaneSweep (planesweep.h:27-510) for callers that bind C:
+ * host images in, host depthmaps out; device buffers are owned by the handle
+ * and reused across calls.  Bool results of the reference map to MVS_OK /
+ * negative codes.  Getters copy into caller memory (the reference returns
+ * pointers to its internal CamImage objects). */
+typedef struct mvs_planesweep mvs_planesweep;
+
+int mvs_ps_create(mvs_planesweep **out);
+int mvs_ps_destroy(mvs_planesweep *ps);
+/* HostRef / HostSrc with their R, t (planesweep.h:31-34, cam_image.h:10-11). */
+int mvs_ps_set_reference(mvs_planesweep *ps, const float *h_img, int32_t width, int32_t height, const float *R9,
+                         const float *t3);
+int mvs_ps_set_sources(mvs_planesweep *ps, const float *h_imgs, int32_t n, const float *R9s, const float *t3s);
+int mvs_ps_set_K(mvs_planesweep *ps, const float *K9);            /* setK */
+int mvs_ps_set_z(mvs_planesweep *ps, float znear, float zfar);     /* setZ */
+int mvs_ps_set_number_of_planes(mvs_planesweep *ps, int32_t n);    /* setNumberofPlanes */
+int mvs_ps_set_number_of_images(mvs_planesweep *ps, int32_t n);    /* setNumberofImages */
+int mvs_ps_set_window_size(mvs_planesweep *ps, int32_t n);         /* setWindowSize (odd only) */
+int mvs_ps_set_std_threshold(mvs_planesweep *ps, float th);        /* setSTDthreshold */
+int mvs_ps_set_ncc_threshold(mvs_planesweep *ps, float th);        /* setNCCthreshold */
+int mvs_ps_set_alternative_relative_matrix_method(mvs_planesweep *ps, int32_t alt);
+/* Extensions: explicit plane list (NULL/0 restores the reference's znear..zfar
+ * float loop), moments/mode/homography precision. */
+int mvs_ps_set_plane_depths(mvs_planesweep *ps, const float *depths, int32_t n);
+int mvs_ps_set_sweep_options(mvs_planesweep *ps, int32_t moments, int32_t mode, int32_t fp64_homographies);
+int mvs_ps_run_algorithm(mvs_planesweep *ps);                      /* RunAlgorithm */
+int mvs_ps_cuda_denoise(mvs_planesweep *ps, int32_t niters, double lambda, double tau, double sigma,
+                        double theta, double beta, double gamma);  /* CudaDenoise */
+int mvs_ps_tgv(mvs_planesweep *ps, int32_t niters, int32_t warps, double lambda, double alpha0, double alpha1,
+               double tau, double sigma, double beta, double gamma); /* TGV (u = 1 start) */
+/* Extension: TGV2 started from the last sweep depthmap (start = 1), from
+ * h_u_init (start = 2) or from 1 (start = 0), with an energy tolerance. */
+int mvs_ps_tgv_ext(mvs_planesweep *ps, const mvs_tgv2_params *params, int32_t start, const float *h_u_init,
+                   int32_t *iters_out, double *energy_out);
+/* Getters (planesweep.h:287-437).  Image getters copy width*height values. */
+int mvs_ps_get_size(mvs_planesweep *ps, int32_t *width, int32_t *height);
+int mvs_ps_get_depthmap(mvs_planesweep *ps, float *out);
+int mvs_ps_get_depthmap8u(mvs_planesweep *ps, uint8_t *out);
+int mvs_ps_get_depthmap_denoised(mvs_planesweep *ps, float *out);
+int mvs_ps_get_depthmap8u_denoised(mvs_planesweep *ps, uint8_t *out);
+int mvs_ps_get_depthmap_tgv(mvs_planesweep *ps, float *out);
+int mvs_ps_get_depthmap8u_tgv(mvs_planesweep *ps, uint8_t *out);
+/* getDepthmapDenoisedPtr: device pointer, overwritten by each CudaDenoise. */
+int mvs_ps_get_depthmap_denoised_ptr(mvs_planesweep *ps, float **d_ptr);
+/* Per-view labels / best NCC of the last sweep (n_views*H*W), extension. */
+int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out);
+int mvs_ps_get_view_best(mvs_planesweep *ps, float *out);
+int mvs_ps_get_3d_coordinates(mvs_planesweep *ps, float *X, float *Y, float *Z); /* get3Dcoordinates */
+int mvs_ps_get_plane_count(mvs_planesweep *ps, int32_t *n);
+/* Device time (ms) of the last run_algorithm / tgv / cuda_denoise call,
+ * measured with CUDA events around the kernels only. */
+int mvs_ps_get_last_kernel_ms(mvs_planesweep *ps, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,57 @@
+// Shared device/host helpers for the sm_100a kernels of libmvs_b200.
+//
+// Every .cu file of the library is compiled with -fmad=false: a plain `a*b+c`
+// is two IEEE roundings, exactly as the reference's arithmetic when it is run
+// on the CPU.  Kernels that want fused multiply-adds on their fast paths ask
+// for them explicitly with fmaf()/__fmaf_rn().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mvs_b200.h"
+
+namespace mvs {
+
+constexpr int kSMs = 148;          // B200: 2 dies x 74 SMs
+constexpr int kMapCamFloats = 21;  // per fusion depthmap: K[9] R[9] t[3]
+
+// Last-error bookkeeping shared by every entry point (defined in capi.cu).
+int set_error(int code, const char *fmt, ...);
+int check_launch(const char *what);
+
+#define MVS_TRY_CUDA(expr)                                                              \
+    do {                                                                                \
+        cudaError_t e__ = (expr);                                                       \
+        if (e__ != cudaSuccess)                                                         \
+            return ::mvs::set_error(MVS_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e__)); \
+    } while (0)
+
+// Boundary mirror of windowed_mean_row/column_kernel (kernels.cu:203-204,
+// 228-229): k < 0 -> -k, k > n-1 -> 2(n-1)-k.  The final clamp only matters
+// for cells that no in-image output reads (entry points reject images
+// narrower than the window, the one case where the reference itself reads
+// out of bounds).
+__device__ __forceinline__ int mirror_idx(int k, int n)
+{
+    if (k < 0) k = -k;
+    if (k > n - 1) k = 2 * (n - 1) - k;
+    return min(max(k, 0), n - 1);
+}
+
+__device__ __forceinline__ float ldg(const float *p) { return __ldg(p); }
+
+// Round-to-nearest-even float -> bf16 bits (finite inputs; NaN stays NaN).
+__device__ __forceinline__ uint16_t f2bf(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+__device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace mvs

@@ -1,0 +1,673 @@
+// Fused plane sweep for sm_100a.
+//
+// One CTA owns a TW x 32 tile of reference pixels for one source view (or,
+// in the aggregated mode, for all views) and walks a chunk of planes.  Per
+// plane it
+//   A0  warps the source over the tile plus its window halo into shared
+//       memory (homography + bilinear, the arithmetic of
+//       transform_indexes_kernel / bilinear_interpolation_kernel_GPU,
+//       kernels.cu:4-44; mirrored halo as windowed_mean_*, kernels.cu:203-229),
+//   A1  forms per-column window sums of w, w^2 and ref*w (64 columns x 4
+//       strips of 8 rows, one per thread; ref values stay in registers),
+//   B   forms the row sums, the NCC (calcNCC_kernel, kernels.cu:46-64) and
+//       keeps the running best per pixel in registers (update_arrays_kernel,
+//       kernels.cu:66-82: strictly greater wins, so ties keep the earlier
+//       plane and NCC <= 0 never wins).
+// This replaces the reference's 12 full-image launches per plane and view
+// (planesweep.cpp:205-249) with two barriers per plane and no HBM traffic
+// except the source gathers (L1/L2 resident) and one result write per pixel.
+//
+// Moments:
+//   MVS_MOMENTS_REFERENCE   the reference's box means (column pass then row
+//                           pass, each sum divided by the window side), its
+//                           naive std and NCC formula, in its operation order;
+//                           with -fmad=false the results are the reference's
+//                           roundings exactly.
+//   MVS_MOMENTS_COMPENSATED window sums of values shifted by a per-tile
+//                           constant (the centre reference value), combined as
+//                           n*Sxx - Sx^2 with a fused multiply-add, so the
+//                           variance does not cancel catastrophically.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace mvs {
+namespace {
+
+constexpr int THREADS = 256;
+constexpr int TH = 32;       // output rows per tile
+constexpr int RWMAX = 64;    // region columns held in shared memory
+constexpr int CSP = 72;      // row pitch of the column-sum arrays (bank spread)
+
+template <int WIN>
+struct Geo {
+    static constexpr int R = WIN / 2;
+    static constexpr int TW = ((RWMAX - 2 * R) / 8) * 8;  // output columns
+    static constexpr int RUN = TW / 8;                     // outputs per thread in pass B
+    static constexpr int RW = TW + 2 * R;                  // region columns used
+    static constexpr int RH = TH + 2 * R;                  // region rows
+    static constexpr int SROWS = 8 + 2 * R;                // region rows per pass-A1 strip
+    static_assert(RW <= RWMAX, "region too wide");
+};
+
+struct SweepArgs {
+    const float *ref;
+    const float *srcs;
+    const float *H;        // [V][P][9]
+    const float *depths;   // [P]
+    int w, h, V, P;
+    int planes_per_chunk;
+    int n_chunks;
+    float stdthresh;
+    unsigned long long *packed;   // PER_VIEW: [V][n] best (ncc bits << 32 | ~plane)
+    unsigned long long *wta;      // AGGREGATED: [n] (cost bits << 32 | plane)
+    uint16_t *cost;               // AGGREGATED: [P][n] bf16 or null
+};
+
+// ---- pass A0: warp one region cell -------------------------------------------
+
+template <int MOM>
+__device__ __forceinline__ float warp_cell(const float *__restrict__ src, int w, int h, const float *Hm, int ix,
+                                           int iy)
+{
+    const float X = (float)(ix + 1), Y = (float)(iy + 1);
+    float xs, ys;
+    if (MOM == MVS_MOMENTS_REFERENCE) {
+        // h * (l+1, k+1, 1), then x / x.z - 1 (kernels.cu:39-40), no contraction
+        const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
+        const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
+        const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
+        xs = q0 / q2 - 1.f;
+        ys = q1 / q2 - 1.f;
+    } else {
+        const float q0 = fmaf(Hm[0], X, fmaf(Hm[1], Y, Hm[2]));
+        const float q1 = fmaf(Hm[3], X, fmaf(Hm[4], Y, Hm[5]));
+        const float q2 = fmaf(Hm[6], X, fmaf(Hm[7], Y, Hm[8]));
+        const float rz = __frcp_rn(q2);
+        xs = fmaf(q0, rz, -1.f);
+        ys = fmaf(q1, rz, -1.f);
+    }
+    const float fx = floorf(xs), fy = floorf(ys);
+    // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
+    if (!(fx >= 0.f && fy >= 0.f && fx + 1.f <= (float)(w - 1) && fy + 1.f <= (float)(h - 1))) return 0.f;
+    const int x0 = (int)fx, y0 = (int)fy;
+    const float a = xs - (float)x0, b = ys - (float)y0;
+    const float *r0 = src + (size_t)y0 * w + x0;
+    const float d00 = ldg(r0), d01 = ldg(r0 + 1), d10 = ldg(r0 + w), d11 = ldg(r0 + w + 1);
+    if (MOM == MVS_MOMENTS_REFERENCE) {
+        const float t1 = a * d01 + (1 - a) * d00;
+        const float t2 = a * d11 + (1 - a) * d10;
+        return b * t2 + (1 - b) * t1;
+    } else {
+        const float t1 = fmaf(a, d01 - d00, d00);
+        const float t2 = fmaf(a, d11 - d10, d10);
+        return fmaf(b, t2 - t1, t1);
+    }
+}
+
+template <int WIN, int MOM>
+__device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h, int x0,
+                                        int y0, const float *Hm)
+{
+    using G = Geo<WIN>;
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        if (rx >= G::RW) continue;
+        const int iy = mirror_idx(y0 - G::R + ry, h), ix = mirror_idx(x0 - G::R + rx, w);
+        Wt[ry][rx] = warp_cell<MOM>(src, w, h, Hm, ix, iy);
+    }
+}
+
+// ---- pass A1: column sums --------------------------------------------------------
+// thread -> (column c = t & 63, strip s = t >> 6 of 8 output rows); refcol holds
+// the strip's reference values (shifted by `shift` in the compensated mode).
+
+template <int WIN, int MOM>
+__device__ __forceinline__ void pass_a1(float (*Wt)[RWMAX], float (*CS)[TH][CSP], const float *refcol, float shift)
+{
+    using G = Geo<WIN>;
+    const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+    if (c >= G::RW) return;
+    float wv[G::SROWS];
+#pragma unroll
+    for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[8 * s + i][c];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
+        if (MOM == MVS_MOMENTS_REFERENCE) {
+            // windowed_mean_column_kernel on warped, warped^2 and ref*warped
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) {
+                const float x = wv[k + i];
+                s1 = s1 + x;
+                s2 = s2 + x * x;
+                s12 = s12 + refcol[k + i] * x;
+            }
+            s1 = s1 / (float)WIN;
+            s2 = s2 / (float)WIN;
+            s12 = s12 / (float)WIN;
+        } else {
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) {
+                const float x = wv[k + i] - shift;
+                s1 += x;
+                s2 = fmaf(x, x, s2);
+                s12 = fmaf(refcol[k + i], x, s12);
+            }
+        }
+        CS[0][8 * s + k][c] = s1;
+        CS[1][8 * s + k][c] = s2;
+        CS[2][8 * s + k][c] = s12;
+    }
+}
+
+// ---- pass B: row sums of the three column-sum arrays ------------------------------
+// thread -> (row y = t >> 3, segment g = t & 7 of RUN outputs)
+
+template <int WIN, int MOM>
+__device__ __forceinline__ void row_sums(float (*CS)[TH][CSP], int q, float *out)
+{
+    using G = Geo<WIN>;
+    const int y = threadIdx.x >> 3, g = threadIdx.x & 7;
+    float v[G::RUN + 2 * G::R];
+#pragma unroll
+    for (int i = 0; i < G::RUN + 2 * G::R; ++i) v[i] = CS[q][y][g * G::RUN + i];
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        float m = 0.f;
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) m = m + v[j + i];
+        out[j] = (MOM == MVS_MOMENTS_REFERENCE) ? m / (float)WIN : m;
+    }
+}
+
+// Reference moments of the tile, once per CTA: in REFERENCE mode the mean and
+// the naive std (calculate_STD_kernel, kernels.cu:103-120) of the reference
+// window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2.
+template <int WIN, int MOM>
+__device__ void ref_moments(float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float *rm, float *rs)
+{
+    using G = Geo<WIN>;
+    {
+        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+        if (c < G::RW) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int i = 0; i < WIN; ++i) {
+                    const float x = (MOM == MVS_MOMENTS_REFERENCE) ? Rt[8 * s + k + i][c]
+                                                                   : Rt[8 * s + k + i][c] - shift;
+                    if (MOM == MVS_MOMENTS_REFERENCE) {
+                        s1 = s1 + x;
+                        s2 = s2 + x * x;
+                    } else {
+                        s1 += x;
+                        s2 = fmaf(x, x, s2);
+                    }
+                }
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    s1 = s1 / (float)WIN;
+                    s2 = s2 / (float)WIN;
+                }
+                CS[0][8 * s + k][c] = s1;
+                CS[1][8 * s + k][c] = s2;
+            }
+        }
+    }
+    __syncthreads();
+    float m[G::RUN], q[G::RUN];
+    row_sums<WIN, MOM>(CS, 0, m);
+    row_sums<WIN, MOM>(CS, 1, q);
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        if (MOM == MVS_MOMENTS_REFERENCE) {
+            const float var = q[j] - m[j] * m[j];
+            rm[j] = m[j];
+            rs[j] = var > 0 ? sqrtf(var) : 0.f;
+        } else {
+            rm[j] = m[j];
+            rs[j] = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
+        }
+    }
+    __syncthreads();
+}
+
+template <int WIN, int MOM>
+__device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm, float rs, float st)
+{
+    if (MOM == MVS_MOMENTS_REFERENCE) {
+        const float var = s2 - s1 * s1;
+        const float sd = var > 0 ? sqrtf(var) : 0.f;
+        if (rs < st || sd < st) return 0.f;
+        return (s12 - rm * s1) / (rs * sd);
+    } else {
+        constexpr float n = (float)(WIN * WIN);
+        const float vx = fmaf(-s1, s1, n * s2);         // n^2 var_w
+        const float cv = fmaf(-s1, rm, n * s12);        // n^2 cov
+        const float thr = st * n;                        // std >= st  <=>  n^2 var >= (st n)^2
+        if (!(vx >= thr * thr) || !(rs >= thr * thr)) return 0.f;
+        return cv * rsqrtf(vx * rs);
+    }
+}
+
+// Shared-memory layout of one CTA.
+struct __align__(16) Smem {
+    float Wt[TH + 16][RWMAX];      // warped region (reference region at start)
+    float CS[3][TH][CSP];          // column sums
+    float Hm[9];
+};
+
+template <int WIN, int MOM>
+__device__ __forceinline__ void load_ref_region(Smem &S, const float *__restrict__ ref, int w, int h, int x0,
+                                                int y0)
+{
+    using G = Geo<WIN>;
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        if (rx >= G::RW) continue;
+        S.Wt[ry][rx] = ldg(ref + (size_t)mirror_idx(y0 - G::R + ry, h) * w + mirror_idx(x0 - G::R + rx, w));
+    }
+}
+
+// ---- per-view kernel -------------------------------------------------------------
+// grid: (tiles_x, tiles_y, V * n_chunks)
+
+template <int WIN, int MOM>
+__global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
+{
+    using G = Geo<WIN>;
+    __shared__ Smem S;
+    const int view = blockIdx.z / a.n_chunks, chunk = blockIdx.z % a.n_chunks;
+    const int x0 = blockIdx.x * G::TW, y0 = blockIdx.y * TH;
+    const int w = a.w, h = a.h;
+    const float *src = a.srcs + (size_t)view * w * h;
+
+    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    __syncthreads();
+    const float shift = (MOM == MVS_MOMENTS_REFERENCE) ? 0.f : S.Wt[G::RH / 2][G::RW / 2];
+    float refcol[G::SROWS];
+    {
+        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+#pragma unroll
+        for (int i = 0; i < G::SROWS; ++i) {
+            const float r = (c < G::RW) ? S.Wt[8 * s + i][c] : 0.f;
+            refcol[i] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+        }
+    }
+    float rm[G::RUN], rs[G::RUN];
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+
+    float best[G::RUN];
+    int lab[G::RUN];
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        best[j] = 0.f;
+        lab[j] = -1;
+    }
+    const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
+    const float *Hv = a.H + (size_t)view * a.P * 9;
+    for (int p = p0; p < p1; ++p) {
+        if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(Hv + (size_t)p * 9 + threadIdx.x);
+        __syncthreads();   // Hm visible; previous plane's pass B finished with CS
+        float Hm[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
+        pass_a0<WIN, MOM>(S.Wt, src, w, h, x0, y0, Hm);
+        __syncthreads();
+        pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
+        __syncthreads();
+        float s1[G::RUN], s2[G::RUN], s12[G::RUN];
+        row_sums<WIN, MOM>(S.CS, 0, s1);
+        row_sums<WIN, MOM>(S.CS, 1, s2);
+        row_sums<WIN, MOM>(S.CS, 2, s12);
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) {
+            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
+            if (c > best[j]) {
+                best[j] = c;
+                lab[j] = p;
+            }
+        }
+    }
+    // results: (ncc bits << 32) | ~plane, so that a 64-bit max keeps the
+    // largest NCC and, among equal NCCs, the earliest plane.
+    const int y = y0 + (threadIdx.x >> 3);
+    if (y >= h) return;
+    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
+    unsigned long long *outp = a.packed + (size_t)view * w * h + (size_t)y * w;
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        const int x = xb + j;
+        if (x >= w) break;
+        unsigned long long key = 0ull;
+        if (lab[j] >= 0)
+            key = ((unsigned long long)__float_as_uint(best[j]) << 32) | (unsigned long long)(0xffffffffu - (unsigned)lab[j]);
+        if (a.n_chunks == 1) outp[x] = key;
+        else if (key) atomicMax(outp + x, key);
+    }
+}
+
+// ---- aggregated kernel: cost = 1 - mean NCC over views, BF16 WTA -------------------
+// grid: (tiles_x, tiles_y, n_chunks)
+
+template <int WIN, int MOM>
+__global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs a)
+{
+    using G = Geo<WIN>;
+    __shared__ Smem S;
+    const int chunk = blockIdx.z;
+    const int x0 = blockIdx.x * G::TW, y0 = blockIdx.y * TH;
+    const int w = a.w, h = a.h;
+    const size_t n = (size_t)w * h;
+
+    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    __syncthreads();
+    const float shift = (MOM == MVS_MOMENTS_REFERENCE) ? 0.f : S.Wt[G::RH / 2][G::RW / 2];
+    float refcol[G::SROWS];
+    {
+        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+#pragma unroll
+        for (int i = 0; i < G::SROWS; ++i) {
+            const float r = (c < G::RW) ? S.Wt[8 * s + i][c] : 0.f;
+            refcol[i] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+        }
+    }
+    float rm[G::RUN], rs[G::RUN];
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+
+    const int y = y0 + (threadIdx.x >> 3);
+    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
+    float bestc[G::RUN];
+    int lab[G::RUN];
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        bestc[j] = 3.f;
+        lab[j] = -1;
+    }
+    const float invV = 1.f / (float)a.V;
+    const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
+    for (int p = p0; p < p1; ++p) {
+        float acc[G::RUN];
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) acc[j] = 0.f;
+        for (int view = 0; view < a.V; ++view) {
+            if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(a.H + ((size_t)view * a.P + p) * 9 + threadIdx.x);
+            __syncthreads();
+            float Hm[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
+            pass_a0<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, x0, y0, Hm);
+            __syncthreads();
+            pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
+            __syncthreads();
+            float s1[G::RUN], s2[G::RUN], s12[G::RUN];
+            row_sums<WIN, MOM>(S.CS, 0, s1);
+            row_sums<WIN, MOM>(S.CS, 1, s2);
+            row_sums<WIN, MOM>(S.CS, 2, s12);
+#pragma unroll
+            for (int j = 0; j < G::RUN; ++j) acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
+        }
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) {
+            const uint16_t cb = f2bf(fmaf(-acc[j], invV, 1.f));
+            const float c = bf2f(cb);
+            const int x = xb + j;
+            if (a.cost && y < h && x < w) a.cost[(size_t)p * n + (size_t)y * w + x] = cb;
+            if (c < bestc[j]) {
+                bestc[j] = c;
+                lab[j] = p;
+            }
+        }
+    }
+    if (y >= h) return;
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        const int x = xb + j;
+        if (x >= w) break;
+        // (cost bits << 32) | plane: a 64-bit min keeps the lowest cost and,
+        // among equal costs, the earliest plane (costs are >= 0).
+        const unsigned long long key = lab[j] < 0 ? ~0ull
+            : ((unsigned long long)__float_as_uint(bestc[j]) << 32) | (unsigned)lab[j];
+        unsigned long long *o = a.wta + (size_t)y * w + x;
+        if (a.n_chunks == 1) *o = key;
+        else if (lab[j] >= 0) atomicMin(o, key);
+    }
+}
+
+// ---- epilogues ----------------------------------------------------------------------
+
+// sum_depthmap_NCC + element_rdivide + set_QNAN_value (kernels.cu:84-101,145-157,
+// 331-340), views in order, float accumulation as the reference.
+__global__ void sweep_combine_kernel(const unsigned long long *__restrict__ packed, const float *__restrict__ depths,
+                                     int n, int V, float nccthresh, float zfar, float *__restrict__ depth,
+                                     int32_t *__restrict__ labels, float *__restrict__ best)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float sum = 0.f, cnt = 0.f;
+        for (int v = 0; v < V; ++v) {
+            const unsigned long long key = packed[(size_t)v * n + i];
+            const int lab = key ? (int)(0xffffffffu - (unsigned)(key & 0xffffffffu)) : -1;
+            const float b = key ? __uint_as_float((unsigned)(key >> 32)) : 0.f;
+            const float d = lab >= 0 ? ldg(depths + lab) : 0.f;
+            if (b > nccthresh) {
+                sum = sum + d;
+                cnt = cnt + 1.f;
+            }
+            if (labels) labels[(size_t)v * n + i] = lab;
+            if (best) best[(size_t)v * n + i] = b;
+        }
+        float r = cnt != 0.f ? sum / cnt : __int_as_float(0x7fc00000);
+        depth[i] = r != r ? zfar : r;
+    }
+}
+
+__global__ void wta_finish_kernel(const unsigned long long *__restrict__ wta, const float *__restrict__ depths, int n,
+                                  float zfar, float *__restrict__ depth, int32_t *__restrict__ labels,
+                                  float *__restrict__ best)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long key = wta[i];
+        const bool ok = key != ~0ull;
+        const int lab = ok ? (int)(unsigned)(key & 0xffffffffu) : -1;
+        depth[i] = ok ? ldg(depths + lab) : zfar;
+        if (labels) labels[i] = lab;
+        if (best) best[i] = ok ? __uint_as_float((unsigned)(key >> 32)) : 3.f;
+    }
+}
+
+// WTA argmin over a stored BF16 cost volume [P][n]: the HBM-bound pass.  Each
+// thread owns 8 consecutive pixels (one 16-byte load per plane).
+__global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restrict__ cost, const float *__restrict__ depths,
+                                                        int n, int P, float zfar, float *__restrict__ depth,
+                                                        int32_t *__restrict__ labels, float *__restrict__ best)
+{
+    const int n8 = n / 8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n8; i += gridDim.x * blockDim.x) {
+        float bc[8];
+        int bl[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            bc[j] = 3.f;
+            bl[j] = -1;
+        }
+        const uint4 *col = reinterpret_cast<const uint4 *>(cost) + i;
+#pragma unroll 4
+        for (int p = 0; p < P; ++p) {
+            const uint4 q = __ldcs(col + (size_t)p * n8);
+            const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float c = bf2f((uint16_t)(wds[j >> 1] >> ((j & 1) * 16)));
+                if (c < bc[j]) {
+                    bc[j] = c;
+                    bl[j] = p;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int k = 8 * i + j;
+            depth[k] = bl[j] >= 0 ? ldg(depths + bl[j]) : zfar;
+            if (labels) labels[k] = bl[j];
+            if (best) best[k] = bc[j];
+        }
+    }
+}
+
+// FP64 homographies: H = K (Rrel + trel e3^T / d) K^-1, H /= H22, for one
+// batch of up to kHomViews views (passed by value: no device allocation).
+constexpr int kHomViews = 32;
+struct HomCams {
+    double K[9], invK[9];
+    double Rrel[kHomViews][9];
+    double trel[kHomViews][3];
+};
+
+__global__ void homography_kernel(HomCams c, const float *__restrict__ depths, int V, int P, float *__restrict__ H)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= V * P) return;
+    const int v = idx / P, p = idx % P;
+    const double d = (double)depths[p];
+    const double *R = c.Rrel[v], *t = c.trel[v];
+    double M[9], T[9], O[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) M[i] = R[i];
+    M[2] += t[0] / d;
+    M[5] += t[1] / d;
+    M[8] += t[2] / d;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = fma(c.K[3 * i], M[j], fma(c.K[3 * i + 1], M[3 + j], c.K[3 * i + 2] * M[6 + j]));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            O[3 * i + j] = fma(T[3 * i], c.invK[j], fma(T[3 * i + 1], c.invK[3 + j], T[3 * i + 2] * c.invK[6 + j]));
+    const double s = O[8];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) H[(size_t)idx * 9 + i] = (float)(O[i] / s);
+}
+
+template <int MOM>
+int launch_window(int win, const SweepArgs &a, int mode, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+#define MVS_SWEEP_CASE(WIN)                                                                          \
+    case WIN: {                                                                                      \
+        dim3 grid(ceil_div(a.w, Geo<WIN>::TW), ceil_div(a.h, TH),                                    \
+                  mode == MVS_SWEEP_PER_VIEW ? a.V * a.n_chunks : a.n_chunks);                       \
+        if (mode == MVS_SWEEP_PER_VIEW) sweep_view_kernel<WIN, MOM><<<grid, THREADS, 0, st>>>(a);   \
+        else sweep_aggregated_kernel<WIN, MOM><<<grid, THREADS, 0, st>>>(a);                        \
+        return check_launch("sweep kernel");                                                         \
+    }
+    switch (win) {
+        MVS_SWEEP_CASE(3)
+        MVS_SWEEP_CASE(5)
+        MVS_SWEEP_CASE(7)
+        MVS_SWEEP_CASE(9)
+        MVS_SWEEP_CASE(11)
+        MVS_SWEEP_CASE(13)
+        MVS_SWEEP_CASE(15)
+    }
+#undef MVS_SWEEP_CASE
+    return set_error(MVS_ERR_ARG, "window %d not supported (odd, 3..15)", win);
+}
+
+int tiles_for(int win, int w, int h)
+{
+    int tw = ((RWMAX - 2 * (win / 2)) / 8) * 8;
+    return ceil_div(w, tw) * ceil_div(h, TH);
+}
+
+}  // namespace
+
+// Plane chunking: enough CTAs for a few waves at 2 CTAs per SM, chunks of at
+// least 16 planes so the per-CTA start-up (reference moments) stays amortised.
+int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode)
+{
+    const int tiles = tiles_for(win, w, h) * (mode == MVS_SWEEP_PER_VIEW ? V : 1);
+    const int target = 4 * 2 * kSMs;
+    int chunks = ceil_div(target, tiles);
+    chunks = max(1, min(chunks, P / 16 > 0 ? P / 16 : 1));
+    return chunks;
+}
+
+int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
+                 float *depth, int32_t *labels, float *best, uint16_t *cost, unsigned long long *scratch,
+                 int n_chunks, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = d->width * d->height;
+    SweepArgs a;
+    a.ref = ref;
+    a.srcs = srcs;
+    a.H = H;
+    a.depths = depths;
+    a.w = d->width;
+    a.h = d->height;
+    a.V = d->n_views;
+    a.P = d->n_planes;
+    a.n_chunks = n_chunks;
+    a.planes_per_chunk = ceil_div(d->n_planes, n_chunks);
+    a.n_chunks = ceil_div(d->n_planes, a.planes_per_chunk);
+    a.stdthresh = d->std_threshold;
+    a.packed = nullptr;
+    a.wta = nullptr;
+    a.cost = nullptr;
+    if (d->mode == MVS_SWEEP_PER_VIEW) {
+        a.packed = scratch;
+        if (a.n_chunks > 1)
+            MVS_TRY_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * (size_t)n * d->n_views, st));
+    } else {
+        a.wta = scratch;
+        a.cost = cost;
+        if (a.n_chunks > 1) MVS_TRY_CUDA(cudaMemsetAsync(scratch, 0xff, sizeof(unsigned long long) * (size_t)n, st));
+    }
+    int rc = d->moments == MVS_MOMENTS_REFERENCE ? launch_window<MVS_MOMENTS_REFERENCE>(d->window, a, d->mode, stream)
+                                                 : launch_window<MVS_MOMENTS_COMPENSATED>(d->window, a, d->mode, stream);
+    if (rc) return rc;
+    const int eb = 256, eg = min(ceil_div(n, eb), 8 * kSMs);
+    if (d->mode == MVS_SWEEP_PER_VIEW) {
+        sweep_combine_kernel<<<eg, eb, 0, st>>>(scratch, depths, n, d->n_views, d->ncc_threshold, d->zfar, depth,
+                                                labels, best);
+    } else {
+        wta_finish_kernel<<<eg, eb, 0, st>>>(scratch, depths, n, d->zfar, depth, labels, best);
+    }
+    return check_launch("sweep epilogue");
+}
+
+int sweep_wta_volume(const uint16_t *cost, const float *depths, int n, int P, float zfar, float *depth,
+                     int32_t *labels, float *best, void *stream)
+{
+    if (n % 8) return set_error(MVS_ERR_ARG, "WTA over a cost volume needs W*H divisible by 8");
+    const int grid = min(ceil_div(n / 8, 256), 16 * kSMs);
+    wta_volume_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(cost, depths, n, P, zfar, depth, labels, best);
+    return check_launch("wta_volume_kernel");
+}
+
+int sweep_homographies(const double *K, const double *invK, const double *Rrel, const double *trel,
+                       const float *depths, int V, int P, float *H, void *stream)
+{
+    for (int v0 = 0; v0 < V; v0 += kHomViews) {
+        const int nv = min(kHomViews, V - v0);
+        HomCams c;
+        for (int i = 0; i < 9; ++i) {
+            c.K[i] = K[i];
+            c.invK[i] = invK[i];
+        }
+        for (int v = 0; v < nv; ++v) {
+            for (int i = 0; i < 9; ++i) c.Rrel[v][i] = Rrel[9 * (v0 + v) + i];
+            for (int i = 0; i < 3; ++i) c.trel[v][i] = trel[3 * (v0 + v) + i];
+        }
+        const int n = nv * P;
+        homography_kernel<<<ceil_div(n, 128), 128, 0, (cudaStream_t)stream>>>(c, depths, nv, P,
+                                                                               H + (size_t)v0 * P * 9);
+    }
+    return check_launch("homography_kernel");
+}
+
+}  // namespace mvs

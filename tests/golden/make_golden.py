@@ -1,0 +1,124 @@
+"""Generate the golden fixtures in tests/golden/*.npz from the reference itself.
+
+The reference's own kernels (kernels.cu, TGV2_kernels.cu, fusion.cu) are
+compiled for the CPU by ``make -C oracle ref`` (oracle/Makefile, shim in
+oracle/ref_shim.h, driver oracle/ref_driver.cpp) and run here on seeded
+synthetic inputs.  Each fixture stores its inputs and the reference's outputs,
+so the tests need neither the reference tree nor the scene generator to agree
+across machines.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT / "plane-sweep-cuda_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+import pyoracle as po  # noqa: E402
+from mvs_b200 import scenes  # noqa: E402
+
+
+def frame_arrays(fr):
+    return dict(ref=fr.ref, srcs=np.stack(fr.srcs), K=fr.ref_cam.K_1based.astype(np.float32),
+                Rref=fr.ref_cam.R.astype(np.float32), tref=fr.ref_cam.t.astype(np.float32),
+                Rsrc=np.stack([c.R for c in fr.src_cams]).astype(np.float32),
+                tsrc=np.stack([c.t for c in fr.src_cams]).astype(np.float32),
+                depth_gt=fr.depth_gt)
+
+
+def poses(a):
+    return [(a["Rsrc"][i], a["tsrc"][i]) for i in range(len(a["Rsrc"]))]
+
+
+def sweep_case(name, seed, w, h, n_src, n_planes, win, planes_kind, znear=0.5, zfar=5.0, nccthresh=0.5):
+    fr, planes, _ = scenes.config_tiny(seed=seed, width=w, height=h, n_src=n_src, n_planes=n_planes, win=win)
+    a = frame_arrays(fr)
+    if planes_kind == "inverse":
+        pl = planes
+        r = po.ref_sweep(a["ref"], list(a["srcs"]), a["K"], a["Rref"], a["tref"], poses(a), pl, win, znear=znear,
+                         zfar=zfar, nccthresh=nccthresh)
+    else:  # the reference's own float loop over [znear, zfar]
+        pl = po.plane_list(znear, zfar, n_planes)
+        r = po.ref_sweep(a["ref"], list(a["srcs"]), a["K"], a["Rref"], a["tref"], poses(a), None, win, znear=znear,
+                         zfar=zfar, nplanes=n_planes, nccthresh=nccthresh)
+    np.savez_compressed(HERE / f"{name}.npz", **a, planes=pl, win=win, znear=znear, zfar=zfar, nccthresh=nccthresh,
+                        stdthresh=1e-4, depth=r["depth"], best=r["best"], vdepth=r["vdepth"],
+                        label=po.labels_from_depth(r["vdepth"], pl))
+
+
+def tgv_case(name, seed, w, h, n_src, niters, warps, start):
+    fr, _, _ = scenes.config_tiny(seed=seed, width=w, height=h, n_src=n_src)
+    a = frame_arrays(fr)
+    u_init = None if start == "one" else a["depth_gt"]
+    u, _ = po.ref_tgv(a["ref"], list(a["srcs"]), a["K"], a["Rref"], a["tref"], poses(a), niters=niters, warps=warps,
+                      u_init=u_init)
+    np.savez_compressed(HERE / f"{name}.npz", **a, niters=niters, warps=warps, start=start, u=u)
+
+
+def tvl1_case(name, seed, w, h, niters):
+    fr, _, _ = scenes.config_tiny(seed=seed, width=w, height=h, n_src=1)
+    rng = np.random.default_rng(seed)
+    d0 = (fr.depth_gt * (1 + 0.02 * rng.standard_normal(fr.depth_gt.shape))).astype(np.float32)
+    znear, zfar = 0.5, 5.0
+    out, _ = po.ref_tvl1_denoise(fr.ref, d0, znear, zfar, niters=niters)
+    np.savez_compressed(HERE / f"{name}.npz", ref=fr.ref, depth_in=d0, znear=znear, zfar=zfar, niters=niters, out=out)
+
+
+def fusion_case(name, seed, dims, bins, n_maps, w, h, iters, interleaved):
+    fi = scenes.fusion_sequence(seed, n_maps, w, h)
+    vol = po.RefVolume(bins, dims, fi.vol_min, fi.vol_max)
+    thr, tau, lam, sigma = 0.05, 0.1, 0.5, 1.0
+    Ks = np.stack([c.K for c in fi.cams]).astype(np.float32)
+    Rs = np.stack([c.R for c in fi.cams]).astype(np.float32)
+    ts = np.stack([c.t for c in fi.cams]).astype(np.float32)
+    depths = np.stack(fi.depths)
+    if interleaved:   # FusionUpdateIteration per map (pclviewer.cpp:1040)
+        for m in range(n_maps):
+            vol.histogram(depths[m], Ks[m], Rs[m], ts[m], thr)
+            vol.update_u(tau, lam)
+            vol.update_p(sigma)
+    else:             # all votes first, then `iters` primal-dual steps
+        for m in range(n_maps):
+            vol.histogram(depths[m], Ks[m], Rs[m], ts[m], thr)
+        hist_only = vol.get()["hist"]
+        for _ in range(iters):
+            vol.update_u(tau, lam)
+            vol.update_p(sigma)
+    g = vol.get()
+    np.savez_compressed(HERE / f"{name}.npz", depths=depths, K=Ks, R=Rs, t=ts, vol_min=fi.vol_min.astype(np.float32),
+                        vol_max=fi.vol_max.astype(np.float32), dims=np.array(dims), bins=bins, thr=thr, tau=tau,
+                        lam=lam, sigma=sigma, iters=iters, interleaved=interleaved, u=g["u"], v=g["v"], p=g["p"],
+                        hist=g["hist"])
+
+
+def main():
+    if po.ref_lib() is None:
+        raise SystemExit("oracle/_ref/libmvs_ref.so is not built (make -C oracle ref)")
+    sweep_case("sweep_inverse_w5", seed=11, w=64, h=48, n_src=2, n_planes=16, win=5, planes_kind="inverse")
+    sweep_case("sweep_refloop_w7", seed=12, w=56, h=40, n_src=3, n_planes=24, win=7, planes_kind="refloop")
+    sweep_case("sweep_inverse_w3_negthr", seed=13, w=40, h=36, n_src=2, n_planes=12, win=3, planes_kind="inverse",
+               nccthresh=-0.25)
+    tgv_case("tgv_from_one", seed=21, w=48, h=40, n_src=2, niters=10, warps=3, start="one")
+    tgv_case("tgv_from_depth", seed=22, w=48, h=40, n_src=3, niters=25, warps=2, start="depth")
+    tvl1_case("tvl1_denoise", seed=31, w=48, h=40, niters=40)
+    fusion_case("fusion_b7_decoupled", seed=41, dims=(20, 16, 12), bins=7, n_maps=3, w=48, h=40, iters=12,
+                interleaved=False)
+    fusion_case("fusion_b8_interleaved", seed=42, dims=(18, 14, 10), bins=8, n_maps=4, w=48, h=40, iters=0,
+                interleaved=True)
+    fusion_case("fusion_b2_decoupled", seed=43, dims=(12, 10, 8), bins=2, n_maps=2, w=40, h=32, iters=6,
+                interleaved=False)
+    fusion_case("fusion_b10_decoupled", seed=44, dims=(12, 10, 8), bins=10, n_maps=3, w=40, h=32, iters=6,
+                interleaved=False)
+    for f in sorted(HERE.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+"""The CPU oracle pinned to the reference (CPU only).
+
+* against the committed golden fixtures (outputs of the reference's own
+  kernels compiled for the CPU by tests/golden/make_golden.py): the f32 oracle
+  is bit-exact, the f64 oracle within stated tolerances;
+* against the reference-on-CPU library live, on fresh seeded inputs, when it
+  was built here (oracle/_ref/libmvs_ref.so).
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from mvs_b200 import scenes
+
+SWEEPS = ["sweep_inverse_w5", "sweep_refloop_w7", "sweep_inverse_w3_negthr"]
+
+
+def poses(g):
+    return [(g["Rsrc"][i], g["tsrc"][i]) for i in range(len(g["Rsrc"]))]
+
+
+@pytest.mark.parametrize("name", SWEEPS)
+def test_sweep_f32_bit_exact_vs_golden(golden, name):
+    g = golden(name)
+    H = po.homographies(g["K"], g["Rref"], g["tref"], poses(g), g["planes"], precision="f32")
+    o = po.sweep(g["ref"], list(g["srcs"]), H, g["planes"], int(g["win"]), nccthresh=float(g["nccthresh"]),
+                 zfar=float(g["zfar"]), precision="f32")
+    np.testing.assert_array_equal(o["best"], g["best"])
+    np.testing.assert_array_equal(o["vdepth"], g["vdepth"])
+    np.testing.assert_array_equal(o["label"], g["label"])
+    np.testing.assert_array_equal(o["depth"], g["depth"])
+
+
+@pytest.mark.parametrize("name", SWEEPS)
+def test_sweep_f64_labels_vs_golden(golden, name):
+    g = golden(name)
+    H = po.homographies(g["K"], g["Rref"], g["tref"], poses(g), g["planes"], precision="f64")
+    o = po.sweep(g["ref"], list(g["srcs"]), H, g["planes"], int(g["win"]), nccthresh=float(g["nccthresh"]),
+                 zfar=float(g["zfar"]), precision="f64")
+    # FP64 moments differ from the reference's naive float moments only where the NCC curve
+    # is flat: the labels agree almost everywhere, and where they differ by more than one
+    # plane the two maxima are equal to float resolution (a tie broken differently).
+    d = np.abs(o["label"] - g["label"])
+    assert np.mean(d == 0) >= 0.995
+    far = d > 1
+    assert np.mean(far) <= 1e-3
+    assert np.all(np.abs(o["best"][far] - g["best"][far]) < 1e-4)
+
+
+def test_reference_plane_loop(golden):
+    g = golden("sweep_refloop_w7")
+    np.testing.assert_array_equal(po.plane_list(float(g["znear"]), float(g["zfar"]), 24), g["planes"])
+    np.testing.assert_array_equal(scenes.reference_plane_list(float(g["znear"]), float(g["zfar"]), 24), g["planes"])
+    # the reference's float loop can drop the last plane (planesweep.cpp:200)
+    assert len(po.plane_list(0.1, 1.0, 200)) == 199
+
+
+@pytest.mark.parametrize("name", ["tgv_from_one", "tgv_from_depth"])
+def test_tgv2_f32_bit_exact_vs_golden(golden, name):
+    g = golden(name)
+    u0 = None if str(g["start"]) == "one" else g["depth_gt"]
+    u, n, _ = po.tgv2(g["ref"], list(g["srcs"]), g["K"], g["Rref"], g["tref"], poses(g), niters=int(g["niters"]),
+                      warps=int(g["warps"]), u_init=u0, precision="f32")
+    np.testing.assert_array_equal(u, g["u"])
+    u64, _, _ = po.tgv2(g["ref"], list(g["srcs"]), g["K"], g["Rref"], g["tref"], poses(g),
+                        niters=int(g["niters"]), warps=int(g["warps"]), u_init=u0, precision="f64")
+    assert np.max(np.abs(u64 - g["u"]) / np.abs(u64)) < 1e-4
+
+
+def test_tvl1_f32_bit_exact_vs_golden(golden):
+    g = golden("tvl1_denoise")
+    o = po.tvl1_denoise(g["ref"], g["depth_in"], float(g["znear"]), float(g["zfar"]), niters=int(g["niters"]),
+                        precision="f32")
+    np.testing.assert_array_equal(o, g["out"])
+
+
+@pytest.mark.parametrize("name", ["fusion_b7_decoupled", "fusion_b8_interleaved", "fusion_b2_decoupled",
+                                  "fusion_b10_decoupled"])
+def test_fusion_f32_bit_exact_vs_golden(golden, name):
+    g = golden(name)
+    v = po.Volume(int(g["bins"]), tuple(g["dims"]), g["vol_min"], g["vol_max"], precision="f32")
+    thr, tau, lam, sigma = float(g["thr"]), float(g["tau"]), float(g["lam"]), float(g["sigma"])
+    if bool(g["interleaved"]):
+        for m in range(len(g["depths"])):
+            v.histogram(g["depths"][m], g["K"][m], g["R"][m], g["t"][m], thr)
+            v.update_u(tau, lam)
+            v.update_p(sigma)
+    else:
+        for m in range(len(g["depths"])):
+            v.histogram(g["depths"][m], g["K"][m], g["R"][m], g["t"][m], thr)
+        for _ in range(int(g["iters"])):
+            v.update_u(tau, lam)
+            v.update_p(sigma)
+    np.testing.assert_array_equal(v.hist, g["hist"])
+    np.testing.assert_array_equal(v.u, g["u"])
+    np.testing.assert_array_equal(v.v, g["v"])
+    np.testing.assert_array_equal(v.p, g["p"])
+
+
+def test_bin_centers():
+    np.testing.assert_array_equal(po.bin_centers(7), np.float32([-1, -1, -0.5, 0, 0.5, 1, 1]))
+    np.testing.assert_array_equal(po.bin_centers(3), np.float32([-1, 0, 1]))
+    np.testing.assert_array_equal(po.bin_centers(2), np.float32([-1, 1]))
+
+
+def prox_closed_form(bins, h, u, tl):
+    """The closed-form median the CUDA U kernel uses (numpy float32 restatement)."""
+    c = po.bin_centers(bins)
+    h = np.asarray(h, np.int64)
+    total = h.sum()
+    pre = np.cumsum(h)
+    B = np.array([max(np.float32(np.float32(u) + np.float32(tl) * np.float32(total - 2 * pre[j - 1])), np.float32(-1))
+                  for j in range(1, bins + 1)], np.float32)[::-1]
+    lo, hi = np.float32(np.inf), np.float32(-np.inf)
+    for i in range(bins + 1):
+        a_lo = c[i - 1] if i > 0 else -np.inf
+        b_lo = B[bins - 1 - i] if bins - 1 - i >= 0 else -np.inf
+        lo = min(lo, max(a_lo, b_lo))
+        a_hi = c[i] if i < bins else np.inf
+        b_hi = B[bins - i] if bins - i < bins else np.inf
+        hi = max(hi, min(a_hi, b_hi))
+    return np.float32(min(max(max(np.float32(u), np.float32(-1)), lo), hi))
+
+
+@pytest.mark.parametrize("bins", [2, 3, 5, 7, 8, 10])
+def test_prox_closed_form_equals_insertion_sort(bins):
+    rng = np.random.default_rng(bins)
+    L = po.oracle_lib()
+    tau, lam = np.float32(0.1), np.float32(0.5)
+    tl = np.float32(tau * lam)
+    for _ in range(400):
+        h = rng.integers(0, 30, bins).astype(np.uint16)
+        if rng.random() < 0.2:
+            h[:] = 0
+        u = np.float32(rng.uniform(-4, 4))
+        want = L.orc_prox_hist_f32(bins, h.ctypes.data_as(po._U16), float(u), float(tau), float(lam))
+        assert prox_closed_form(bins, h, u, tl) == np.float32(want)
+
+
+needs_ref = pytest.mark.skipif(po.ref_lib() is None, reason="reference-on-CPU library not built here")
+
+
+@needs_ref
+def test_live_sweep_vs_reference():
+    fr, planes, win = scenes.config_tiny(seed=101, width=72, height=50, n_src=3, n_planes=20, win=9)
+    p = [(c.R, c.t) for c in fr.src_cams]
+    r = po.ref_sweep(fr.ref, fr.srcs, fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, p, planes, win, zfar=5.0)
+    H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, p, planes, precision="f32")
+    o = po.sweep(fr.ref, fr.srcs, H, planes, win, zfar=5.0, precision="f32")
+    np.testing.assert_array_equal(o["depth"], r["depth"])
+    np.testing.assert_array_equal(o["best"], r["best"])
+
+
+@needs_ref
+def test_live_fusion_and_tgv_vs_reference():
+    fi = scenes.fusion_sequence(102, 2, 40, 30)
+    rv = po.RefVolume(6, (14, 12, 10), fi.vol_min, fi.vol_max)
+    ov = po.Volume(6, (14, 12, 10), fi.vol_min, fi.vol_max, precision="f32")
+    for d, c in zip(fi.depths, fi.cams):
+        rv.histogram(d, c.K, c.R, c.t, 0.07)
+        ov.histogram(d, c.K, c.R, c.t, 0.07)
+    for _ in range(5):
+        rv.update_u(0.1, 0.5), rv.update_p(1.0)
+        ov.update_u(0.1, 0.5), ov.update_p(1.0)
+    got = rv.get()
+    np.testing.assert_array_equal(got["hist"], ov.hist)
+    np.testing.assert_array_equal(got["u"], ov.u)
+    fr, _, _ = scenes.config_tiny(seed=103, width=40, height=32, n_src=2)
+    p = [(c.R, c.t) for c in fr.src_cams]
+    ur, _ = po.ref_tgv(fr.ref, fr.srcs, fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, p, niters=7, warps=2,
+                       beta=1.5, gamma=0.8)
+    uo, _, _ = po.tgv2(fr.ref, fr.srcs, fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, p, niters=7, warps=2,
+                       beta=1.5, gamma=0.8, precision="f32")
+    np.testing.assert_array_equal(ur, uo)

@@ -1,0 +1,116 @@
+"""TGV2, TV-L1 denoise and compute3D on the GPU against the reference and the oracle.
+
+The fused kernels perform the reference's arithmetic statement for statement,
+so against the reference's own kernels (golden fixtures, run on the CPU) the
+results are bit-identical; against the FP64 oracle the stated bar is 1e-4
+relative on the depth.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import mvs_b200 as M
+from mvs_b200 import hostmath as hm, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def tgv_inputs(g):
+    K = g["K"]
+    rel = [hm.relative_f32(g["Rref"], g["tref"], g["Rsrc"][i], g["tsrc"][i]) for i in range(len(g["Rsrc"]))]
+    invK = hm.inv3_f32(K)
+    Rs = np.stack([r[0].reshape(9) for r in rel])
+    ts = np.stack([r[1] for r in rel])
+    return np.float32(K).reshape(9), invK.reshape(9), Rs, ts
+
+
+def run_tgv(cuda, ref, srcs, K9, iK9, Rs, ts, params, u0=None):
+    import torch
+    h, w = ref.shape
+    V = len(srcs)
+    d_ref = torch.from_numpy(np.ascontiguousarray(ref, np.float32)).to(cuda)
+    d_srcs = torch.from_numpy(np.ascontiguousarray(np.stack(srcs), np.float32)).to(cuda)
+    u = torch.empty((h, w), dtype=torch.float32, device=cuda)
+    if u0 is not None:
+        u.copy_(torch.from_numpy(np.ascontiguousarray(u0, np.float32)))
+    ws = torch.empty(M.tgv2_workspace_bytes(w, h, V) // 8 + 1, dtype=torch.int64, device=cuda)
+    it, e = M.tgv2_run(d_ref, d_srcs, K9, iK9, Rs, ts, params, u, u_from_input=u0 is not None, workspace=ws)
+    torch.cuda.synchronize()
+    return u.cpu().numpy(), it, e
+
+
+@pytest.mark.parametrize("name", ["tgv_from_one", "tgv_from_depth"])
+def test_tgv2_bit_exact_vs_reference(cuda, golden, name):
+    g = golden(name)
+    K9, iK9, Rs, ts = tgv_inputs(g)
+    p = M.tgv2_params(niters=int(g["niters"]), warps=int(g["warps"]))
+    u0 = None if str(g["start"]) == "one" else g["depth_gt"]
+    u, it, _ = run_tgv(cuda, g["ref"], list(g["srcs"]), K9, iK9, Rs, ts, p, u0)
+    assert it == int(g["niters"]) * int(g["warps"])
+    np.testing.assert_array_equal(u, g["u"])
+
+
+def test_tgv2_tolerance_vs_fp64_oracle(cuda):
+    """TGV2 from a noisy start to relative energy change 1e-4: the FP64 oracle stops within one
+    check of the GPU, and at the GPU's iteration count the depth and the energy agree within
+    1e-4 relative."""
+    fr, planes, win = scenes.config_tiny(seed=4, width=80, height=60, n_src=3, n_planes=16, win=5)
+    rng = np.random.default_rng(4)
+    u0 = (fr.depth_gt * (1 + 0.01 * rng.standard_normal(fr.depth_gt.shape))).astype(np.float32)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    g = dict(K=np.float32(K1), Rref=fr.ref_cam.R, tref=fr.ref_cam.t, Rsrc=np.stack([c.R for c in fr.src_cams]),
+             tsrc=np.stack([c.t for c in fr.src_cams]))
+    K9, iK9, Rs, ts = tgv_inputs(g)
+    p = M.tgv2_params(niters=300, warps=1, tol=1e-4, check_every=10)
+    u, it, e = run_tgv(cuda, fr.ref, fr.srcs, K9, iK9, Rs, ts, p, u0)
+    _, ito, _ = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=300, warps=1, u_init=u0,
+                        precision="f64", tol=1e-4, check_every=10)
+    assert 0 < it < 300 and abs(it - ito) <= 10, (it, ito)
+    uo, _, eo = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=it, warps=1, u_init=u0,
+                        precision="f64", tol=1e-30, check_every=it)
+    assert abs(e - eo[-1]) <= 1e-4 * abs(eo[-1]), (e, eo[-1])
+    rel = np.abs(u - uo) / np.abs(uo)
+    assert rel.max() <= 1e-4, rel.max()
+
+
+def test_tvl1_denoise_bit_exact_vs_reference(cuda, golden):
+    import torch
+    g = golden("tvl1_denoise")
+    h, w = g["depth_in"].shape
+    d_ref = torch.from_numpy(g["ref"]).to(cuda)
+    d = torch.from_numpy(g["depth_in"].copy()).to(cuda)
+    ws = torch.empty(M.tvl1_workspace_bytes(w, h) // 8 + 1, dtype=torch.int64, device=cuda)
+    M.tvl1_denoise(d_ref, d, float(g["znear"]), float(g["zfar"]), M.tvl1_params(niters=int(g["niters"])), ws)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), g["out"])
+
+
+def test_compute3d_matches_reference(cuda):
+    import torch
+    fr, _, _ = scenes.config_tiny(seed=6, width=40, height=30, n_src=1)
+    L = po.ref_lib()
+    K = np.float32(fr.ref_cam.K_1based)
+    R = np.float32(fr.ref_cam.R)
+    t = np.float32(fr.ref_cam.t)
+    depth = fr.depth_gt.copy()
+    depth[0, :5] = 7.0                         # beyond the 5.5 cut-off
+    # camera -> world as get3Dcoordinates builds it: RelativeMatrices(ref, I)
+    Rr, tr = hm.relative_f32(R, t, np.eye(3, dtype=np.float32), np.zeros(3, np.float32))
+    d = torch.from_numpy(depth).to(cuda)
+    X = torch.zeros_like(d)
+    Y = torch.zeros_like(d)
+    Z = torch.empty_like(d)
+    M.compute3d(d, hm.inv3_f32(K).reshape(9), Rr.reshape(9), tr, X, Y, Z)
+    torch.cuda.synchronize()
+    o = [np.zeros_like(depth) for _ in range(3)]
+    po.oracle_lib().orc_compute3d_f32(40, 30, po._fp(depth), po._fp(hm.inv3_f32(K).reshape(9).copy()),
+                                      po._fp(Rr.reshape(9).copy()), po._fp(tr.copy()), *[po._fp(a) for a in o])
+    np.testing.assert_array_equal(X.cpu().numpy(), o[0])
+    np.testing.assert_array_equal(Y.cpu().numpy(), o[1])
+    np.testing.assert_array_equal(Z.cpu().numpy(), o[2])
+    if L is not None:   # also the reference's own kernel, when built here
+        rx, ry, rz = (np.zeros_like(depth) for _ in range(3))
+        L.ref_compute3d(40, 30, po._fp(depth), po._fp(K.reshape(9).copy()), po._fp(R.reshape(9).copy()),
+                        po._fp(t.copy()), 0, po._fp(rx), po._fp(ry), po._fp(rz))
+        np.testing.assert_array_equal(Z.cpu().numpy(), rz)

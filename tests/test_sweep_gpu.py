@@ -1,0 +1,255 @@
+"""Plane sweep on the GPU against the reference and the oracle.
+
+Parity bars (stated per output):
+* reference arithmetic (MVS_MOMENTS_REFERENCE) fed the reference's float
+  homographies: per-view best NCC, labels and the averaged depthmap are
+  bit-identical to the reference's own kernels run on the CPU;
+* FP64 homographies built on the device: per-view labels identical on
+  >= 99.9% of pixels and within one plane elsewhere;
+* compensated moments: labels against the FP64 oracle, same bar.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import mvs_b200 as M
+from mvs_b200 import hostmath as hm, scenes
+
+pytestmark = pytest.mark.gpu
+
+SWEEP_GOLDEN = ["sweep_inverse_w5", "sweep_refloop_w7", "sweep_inverse_w3_negthr"]
+
+
+def float_H(K, Rref, tref, poses, planes):
+    invK = hm.inv3_f32(K)
+    out = []
+    for Rs, ts in poses:
+        Rrel, trel = hm.relative_f32(Rref, tref, Rs, ts)
+        out.append([hm.homography_f32(np.float32(K), invK, Rrel, trel, d).reshape(9) for d in planes])
+    return np.asarray(out, np.float32)
+
+
+def run_sweep(cuda, ref, srcs, planes, win, K=None, Rref=None, tref=None, poses=None, H=None,
+              moments=M.MOMENTS_REFERENCE, mode=M.SWEEP_PER_VIEW, nccthresh=0.5, zfar=5.0, cost=False):
+    import torch
+    h, w = ref.shape
+    V, P = len(srcs), len(planes)
+    desc = M.sweep_desc(w, h, V, P, win, moments, mode, 1e-4, nccthresh, zfar)
+    d_ref = torch.from_numpy(np.ascontiguousarray(ref, np.float32)).to(cuda)
+    d_srcs = torch.from_numpy(np.ascontiguousarray(np.stack(srcs), np.float32)).to(cuda)
+    d_depths = torch.from_numpy(np.ascontiguousarray(planes, np.float32)).to(cuda)
+    if H is None:
+        rel = [M.relative_pose(Rref, tref, Rs, ts) for Rs, ts in poses]
+        d_H = torch.empty(V * P * 9, dtype=torch.float32, device=cuda)
+        M.sweep_homographies(desc, K, rel, d_depths, d_H)
+    else:
+        d_H = torch.from_numpy(np.ascontiguousarray(H, np.float32)).to(cuda)
+    nl = V if mode == M.SWEEP_PER_VIEW else 1
+    depth = torch.empty((h, w), dtype=torch.float32, device=cuda)
+    labels = torch.empty((nl, h, w), dtype=torch.int32, device=cuda)
+    best = torch.empty((nl, h, w), dtype=torch.float32, device=cuda)
+    d_cost = torch.empty((P, h, w), dtype=torch.int16, device=cuda) if cost else None
+    ws = torch.empty(M.sweep_workspace_bytes(desc) // 8 + 1, dtype=torch.int64, device=cuda)
+    M.sweep(desc, d_ref, d_srcs, d_H, d_depths, depth, labels, best, d_cost, ws)
+    torch.cuda.synchronize()
+    out = dict(depth=depth.cpu().numpy(), label=labels.cpu().numpy(), best=best.cpu().numpy(), H=d_H.cpu().numpy())
+    if cost:
+        out["cost"] = d_cost.cpu().numpy().view(np.uint16)
+    return out
+
+
+def label_agreement(a, b):
+    same = float(np.mean(a == b))
+    near = float(np.mean(np.abs(a.astype(np.int64) - b.astype(np.int64)) <= 1))
+    return same, near
+
+
+@pytest.mark.parametrize("name", SWEEP_GOLDEN)
+def test_reference_arithmetic_bit_exact_vs_reference(cuda, golden, name):
+    g = golden(name)
+    poses = [(g["Rsrc"][i], g["tsrc"][i]) for i in range(len(g["Rsrc"]))]
+    H = float_H(g["K"], g["Rref"], g["tref"], poses, g["planes"])
+    r = run_sweep(cuda, g["ref"], list(g["srcs"]), g["planes"], int(g["win"]), H=H, nccthresh=float(g["nccthresh"]),
+                  zfar=float(g["zfar"]))
+    np.testing.assert_array_equal(r["best"], g["best"])
+    np.testing.assert_array_equal(r["label"], g["label"])
+    np.testing.assert_array_equal(r["depth"], g["depth"])
+
+
+def assert_label_parity(lab, best, ref_lab, ref_best, same_min=0.999):
+    """Labels identical on >= same_min of the pixels; elsewhere within one plane, except
+    ties: where the labels are further apart the two best NCCs agree to 1e-4."""
+    d = np.abs(lab.astype(np.int64) - ref_lab.astype(np.int64))
+    same = float(np.mean(d == 0))
+    far = d > 1
+    assert same >= same_min, (same, float(np.mean(far)))
+    assert np.all(np.abs(best[far] - ref_best[far]) < 1e-4), float(np.mean(far))
+    return same
+
+
+@pytest.mark.parametrize("name", SWEEP_GOLDEN)
+def test_fp64_homographies_label_parity(cuda, golden, name):
+    g = golden(name)
+    poses = [(g["Rsrc"][i], g["tsrc"][i]) for i in range(len(g["Rsrc"]))]
+    r = run_sweep(cuda, g["ref"], list(g["srcs"]), g["planes"], int(g["win"]), K=g["K"].astype(np.float64),
+                  Rref=g["Rref"], tref=g["tref"], poses=poses, nccthresh=float(g["nccthresh"]), zfar=float(g["zfar"]))
+    assert_label_parity(r["label"], r["best"], g["label"], g["best"], same_min=0.995)
+    # the device homographies agree with the reference's float ones to float precision
+    Hf = float_H(g["K"], g["Rref"], g["tref"], poses, g["planes"]).reshape(-1, 9)
+    np.testing.assert_allclose(r["H"].reshape(-1, 9), Hf, rtol=2e-5, atol=2e-5)
+
+
+def test_c1_fp64_homographies_label_parity(cuda):
+    """320x240, 4 views, 64 planes, 7x7 with FP64 device homographies against the reference's
+    arithmetic (f32 oracle, bit-exact with the reference): >= 99.9% identical labels."""
+    fr, planes, win = scenes.config_small(seed=1)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    H = po.homographies(K1, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f32")
+    o = po.sweep(fr.ref, fr.srcs, H, planes, win, zfar=5.0, precision="f32")
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, K=K1, Rref=fr.ref_cam.R, tref=fr.ref_cam.t, poses=poses,
+                  zfar=5.0)
+    assert_label_parity(r["label"], r["best"], o["label"], o["best"], same_min=0.999)
+
+
+def test_c1_size_reference_arithmetic_bit_exact(cuda):
+    """320x240, 4 views, 64 inverse-depth planes, 7x7: the GPU equals the f32 oracle bit for bit."""
+    fr, planes, win = scenes.config_small(seed=1)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    H = po.homographies(K1, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f32")
+    o = po.sweep(fr.ref, fr.srcs, H, planes, win, zfar=5.0, precision="f32")
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, H=H, zfar=5.0)
+    np.testing.assert_array_equal(r["best"], o["best"])
+    np.testing.assert_array_equal(r["label"], o["label"])
+    np.testing.assert_array_equal(r["depth"], o["depth"])
+
+
+def test_c1_compensated_vs_fp64_oracle(cuda):
+    fr, planes, win = scenes.config_small(seed=1)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    H64 = po.homographies(K1, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f64")
+    o = po.sweep(fr.ref, fr.srcs, H64, planes, win, zfar=5.0, precision="f64")
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, K=K1, Rref=fr.ref_cam.R, tref=fr.ref_cam.t, poses=poses,
+                  moments=M.MOMENTS_COMPENSATED, zfar=5.0)
+    assert_label_parity(r["label"], r["best"], o["label"], o["best"], same_min=0.999)
+    # NCC of the winning plane within 1e-4 where both agree on the plane
+    m = r["label"] == o["label"]
+    assert np.max(np.abs(r["best"][m] - o["best"][m])) < 1e-4
+
+
+def bf16_round(x):
+    x = np.ascontiguousarray(x, np.float32)
+    u = x.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return (u.astype(np.uint32) << 16).view(np.float32)
+
+
+def test_aggregated_bf16_wta_vs_fp64_oracle(cuda):
+    fr, planes, win = scenes.config_tiny(seed=5, width=96, height=64, n_src=3, n_planes=24, win=7)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    H64 = po.homographies(K1, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f64")
+    L = po.oracle_lib()
+    h, w = fr.ref.shape
+    ncc = np.zeros((len(poses), len(planes), h, w))
+    for v in range(len(poses)):
+        for p in range(len(planes)):
+            buf = np.zeros((h, w))
+            L.orc_sweep_ncc_f64(w, h, po._fp(po._f32(fr.ref)), po._fp(po._f32(fr.srcs[v])),
+                                po._dp(np.ascontiguousarray(H64[v, p])), win, 1e-4, po._dp(buf))
+            ncc[v, p] = buf
+    cost = bf16_round((1.0 - ncc.mean(0)).astype(np.float32))
+    lab = np.argmin(cost, axis=0)
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, K=K1, Rref=fr.ref_cam.R, tref=fr.ref_cam.t, poses=poses,
+                  moments=M.MOMENTS_COMPENSATED, mode=M.SWEEP_AGGREGATED, zfar=5.0, cost=True)
+    same, near = label_agreement(r["label"][0], lab)
+    assert same >= 0.99 and near >= 0.999, (same, near)
+    # the stored cost volume and a separate WTA pass over it give the same labels
+    gpu_cost = (r["cost"].astype(np.uint32) << 16).view(np.float32)
+    assert np.max(np.abs(gpu_cost - cost)) <= 0.02
+    np.testing.assert_array_equal(np.argmin(gpu_cost, axis=0), r["label"][0])
+
+
+def test_wta_volume_kernel(cuda):
+    import torch
+    rng = np.random.default_rng(0)
+    P, h, w = 37, 24, 40
+    cost = bf16_round(rng.random((P, h, w), dtype=np.float32) * 2)
+    cost[5, 3, 7] = cost[:, 3, 7].min()          # a tie: the earlier plane wins
+    bits = (cost.view(np.uint32) >> 16).astype(np.uint16)
+    depths = np.linspace(1, 2, P).astype(np.float32)
+    d_cost = torch.from_numpy(bits.view(np.int16)).to(cuda)
+    d_depths = torch.from_numpy(depths).to(cuda)
+    depth = torch.empty((h, w), device=cuda)
+    labels = torch.empty((h, w), dtype=torch.int32, device=cuda)
+    best = torch.empty((h, w), device=cuda)
+    M.sweep_wta_volume(d_cost, d_depths, h * w, P, 9.0, depth, labels, best)
+    torch.cuda.synchronize()
+    lab = np.argmin(cost, axis=0)
+    np.testing.assert_array_equal(labels.cpu().numpy(), lab)
+    np.testing.assert_array_equal(depth.cpu().numpy(), depths[lab])
+
+
+@pytest.mark.parametrize("win", [3, 9, 15])
+def test_window_sizes_and_ragged_tiles(cuda, win):
+    """Odd sizes that do not divide the tile; image only slightly larger than the window."""
+    fr, planes, _ = scenes.config_tiny(seed=7, width=win + 5, height=win + 2, n_src=2, n_planes=9, win=win)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f32")
+    o = po.sweep(fr.ref, fr.srcs, H, planes, win, zfar=5.0, precision="f32")
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, H=H, zfar=5.0)
+    np.testing.assert_array_equal(r["best"], o["best"])
+    np.testing.assert_array_equal(r["label"], o["label"])
+    np.testing.assert_array_equal(r["depth"], o["depth"])
+
+
+def test_flat_source_gives_no_match_and_zfar(cuda):
+    """A constant source has zero window std: NCC is 0 everywhere, no plane wins, depth = zfar."""
+    fr, planes, win = scenes.config_tiny(seed=8, width=48, height=40, n_src=2, n_planes=6, win=5)
+    srcs = [np.full_like(fr.srcs[0], 77.0), np.full_like(fr.srcs[1], 12.5)]
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f32")
+    r = run_sweep(cuda, fr.ref, srcs, planes, win, H=H, zfar=3.25)
+    assert np.all(r["label"] == -1)
+    assert np.all(r["best"] == 0)
+    assert np.all(r["depth"] == np.float32(3.25))
+
+
+def test_many_plane_chunks_match_single_chunk(cuda):
+    """A small image with many planes is split into plane chunks merged by 64-bit max; same result."""
+    fr, _, win = scenes.config_tiny(seed=9, width=40, height=32, n_src=1, n_planes=8, win=5)
+    planes = scenes.inverse_depth_planes(0.5, 5.0, 300)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f32")
+    o = po.sweep(fr.ref, fr.srcs, H, planes, win, zfar=5.0, precision="f32")
+    r = run_sweep(cuda, fr.ref, fr.srcs, planes, win, H=H, zfar=5.0)
+    np.testing.assert_array_equal(r["label"], o["label"])
+    np.testing.assert_array_equal(r["best"], o["best"])
+
+
+def test_full_size_properties(cuda):
+    """640x480, 8 views, 256 planes, 9x9 (compensated): labels in range, deterministic, depth
+    consistent with the per-view labels, and close to the ray-cast ground truth."""
+    fr, planes, win = scenes.config_full(seed=2)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    args = dict(K=fr.ref_cam.K_1based, Rref=fr.ref_cam.R, tref=fr.ref_cam.t, poses=poses,
+                moments=M.MOMENTS_COMPENSATED, zfar=8.0)
+    r1 = run_sweep(cuda, fr.ref, fr.srcs, planes, win, **args)
+    r2 = run_sweep(cuda, fr.ref, fr.srcs, planes, win, **args)
+    np.testing.assert_array_equal(r1["label"], r2["label"])
+    np.testing.assert_array_equal(r1["depth"], r2["depth"])
+    lab = r1["label"]
+    assert lab.min() >= -1 and lab.max() < len(planes)
+    # the averaged depth is the reference combine of the per-view labels
+    vd = np.where(lab >= 0, planes[np.clip(lab, 0, None)], 0).astype(np.float32)
+    ok = r1["best"] > 0.5
+    cnt = ok.sum(0).astype(np.float32)
+    s = np.zeros(fr.ref.shape, np.float32)
+    for v in range(len(poses)):
+        s = (s + np.where(ok[v], vd[v], 0)).astype(np.float32)
+    want = np.where(cnt > 0, s / np.where(cnt > 0, cnt, 1), 8.0).astype(np.float32)
+    np.testing.assert_allclose(r1["depth"], want, rtol=1e-6)
+    rel = np.abs(r1["depth"] - fr.depth_gt) / fr.depth_gt
+    assert np.median(rel[cnt > 0]) < 0.03
