@@ -125,9 +125,9 @@ def cpu_reference_sample(fr, planes, n_planes_sample=4):
                          zfar=8.0)
         secs, kind, cores = r["seconds"], "reference", os.cpu_count()
     else:
-        H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, sample, precision="f32")
+        Hs = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, sample, precision="f32")
         t0 = time.perf_counter()
-        po.sweep(fr.ref, fr.srcs, H, sample, WIN, zfar=8.0, precision="f32")
+        po.sweep(fr.ref, fr.srcs, Hs, sample, WIN, zfar=8.0, precision="f32")
         secs, kind, cores = time.perf_counter() - t0, "port", 1
     evals = W * H * V * len(sample)
     return evals / secs / 1e6, secs, kind, cores, f"640x480 frame, 8 views, {len(sample)} of the 256 planes, 9x9"

@@ -249,7 +249,7 @@ protected:
     bool depthavailable = false, alternativemethod = false;
     std::vector<float> planelist, lastplanes;
     int sweepmoments = MVS_MOMENTS_REFERENCE, sweepmode = MVS_SWEEP_PER_VIEW;
-    bool fp64homography = true;
+    bool fp64homography = false;   /* reference-float homographies: bit-exact with the reference */
     std::vector<int32_t> viewlabels;
     std::vector<float> viewbest;
     float lastms = 0.f;

@@ -51,9 +51,11 @@ def test_tgv2_bit_exact_vs_reference(cuda, golden, name):
 
 
 def test_tgv2_tolerance_vs_fp64_oracle(cuda):
-    """TGV2 from a noisy start to relative energy change 1e-4: the FP64 oracle stops within one
-    check of the GPU, and at the GPU's iteration count the depth and the energy agree within
-    1e-4 relative."""
+    """TGV2 from a noisy start with an energy tolerance: the FP64 oracle stops within one check
+    of the GPU, and at the GPU's iteration count the depth and the energy agree within 1e-4
+    relative.  (With the reference's step sizes, tau = 0.02 and sigma = 1, the relative
+    energy change per 10 iterations stays near 1e-3 for hundreds of iterations, so a 3e-3
+    tolerance is used to exercise the stopping rule on a small frame.)"""
     fr, planes, win = scenes.config_tiny(seed=4, width=80, height=60, n_src=3, n_planes=16, win=5)
     rng = np.random.default_rng(4)
     u0 = (fr.depth_gt * (1 + 0.01 * rng.standard_normal(fr.depth_gt.shape))).astype(np.float32)
@@ -62,10 +64,10 @@ def test_tgv2_tolerance_vs_fp64_oracle(cuda):
     g = dict(K=np.float32(K1), Rref=fr.ref_cam.R, tref=fr.ref_cam.t, Rsrc=np.stack([c.R for c in fr.src_cams]),
              tsrc=np.stack([c.t for c in fr.src_cams]))
     K9, iK9, Rs, ts = tgv_inputs(g)
-    p = M.tgv2_params(niters=300, warps=1, tol=1e-4, check_every=10)
+    p = M.tgv2_params(niters=300, warps=1, tol=3e-3, check_every=10)
     u, it, e = run_tgv(cuda, fr.ref, fr.srcs, K9, iK9, Rs, ts, p, u0)
     _, ito, _ = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=300, warps=1, u_init=u0,
-                        precision="f64", tol=1e-4, check_every=10)
+                        precision="f64", tol=3e-3, check_every=10)
     assert 0 < it < 300 and abs(it - ito) <= 10, (it, ito)
     uo, _, eo = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=it, warps=1, u_init=u0,
                         precision="f64", tol=1e-30, check_every=it)
