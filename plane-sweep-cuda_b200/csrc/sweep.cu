@@ -24,9 +24,14 @@
 //                           with -fmad=false the results are the reference's
 //                           roundings exactly.
 //   MVS_MOMENTS_COMPENSATED window sums of values shifted by a per-tile
-//                           constant (the centre reference value), combined as
-//                           n*Sxx - Sx^2 with a fused multiply-add, so the
-//                           variance does not cancel catastrophically.
+//                           constant (the mean of the tile's reference region),
+//                           kept as sliding sums and combined as n*Sxx - Sx^2
+//                           with a fused multiply-add, so the variance does not
+//                           cancel catastrophically.  A window whose n*Sxx - Sx^2
+//                           is within the rounding bound of the sums
+//                           (kappa * Sxx) counts as flat (std 0): constant
+//                           windows, such as the zero fill outside the source,
+//                           then give NCC 0 exactly as in exact arithmetic.
 #include <math.h>
 
 #include "common.cuh"
@@ -64,57 +69,93 @@ struct SweepArgs {
     uint16_t *cost;               // AGGREGATED: [P][n] bf16 or null
 };
 
-// ---- pass A0: warp one region cell -------------------------------------------
+// ---- pass A0: warp the region into shared memory ------------------------------
 
-template <int MOM>
-__device__ __forceinline__ float warp_cell(const float *__restrict__ src, int w, int h, const float *Hm, int ix,
-                                           int iy)
-{
-    const float X = (float)(ix + 1), Y = (float)(iy + 1);
-    float xs, ys;
-    if (MOM == MVS_MOMENTS_REFERENCE) {
-        // h * (l+1, k+1, 1), then x / x.z - 1 (kernels.cu:39-40), no contraction
-        const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
-        const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
-        const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
-        xs = q0 / q2 - 1.f;
-        ys = q1 / q2 - 1.f;
-    } else {
-        const float q0 = fmaf(Hm[0], X, fmaf(Hm[1], Y, Hm[2]));
-        const float q1 = fmaf(Hm[3], X, fmaf(Hm[4], Y, Hm[5]));
-        const float q2 = fmaf(Hm[6], X, fmaf(Hm[7], Y, Hm[8]));
-        const float rz = __frcp_rn(q2);
-        xs = fmaf(q0, rz, -1.f);
-        ys = fmaf(q1, rz, -1.f);
-    }
-    const float fx = floorf(xs), fy = floorf(ys);
-    // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
-    if (!(fx >= 0.f && fy >= 0.f && fx + 1.f <= (float)(w - 1) && fy + 1.f <= (float)(h - 1))) return 0.f;
-    const int x0 = (int)fx, y0 = (int)fy;
-    const float a = xs - (float)x0, b = ys - (float)y0;
-    const float *r0 = src + (size_t)y0 * w + x0;
-    const float d00 = ldg(r0), d01 = ldg(r0 + 1), d10 = ldg(r0 + w), d11 = ldg(r0 + w + 1);
-    if (MOM == MVS_MOMENTS_REFERENCE) {
-        const float t1 = a * d01 + (1 - a) * d00;
-        const float t2 = a * d11 + (1 - a) * d10;
-        return b * t2 + (1 - b) * t1;
-    } else {
-        const float t1 = fmaf(a, d01 - d00, d00);
-        const float t2 = fmaf(a, d11 - d10, d10);
-        return fmaf(b, t2 - t1, t1);
-    }
-}
-
+// Cells are processed in batches: all coordinates of a batch first, then all
+// of its gathers, then the interpolation, so that each thread keeps several
+// independent L1/L2 gathers in flight.
 template <int WIN, int MOM>
 __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h, int x0,
                                         int y0, const float *Hm)
 {
     using G = Geo<WIN>;
-    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
-        const int ry = i / RWMAX, rx = i % RWMAX;
-        if (rx >= G::RW) continue;
-        const int iy = mirror_idx(y0 - G::R + ry, h), ix = mirror_idx(x0 - G::R + rx, w);
-        Wt[ry][rx] = warp_cell<MOM>(src, w, h, Hm, ix, iy);
+    constexpr int CELLS = (G::RH * RWMAX + THREADS - 1) / THREADS;
+    constexpr int BATCH = 4;
+#pragma unroll
+    for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
+        float fa[BATCH], fb[BATCH];
+        int off[BATCH];
+        bool in[BATCH], ok[BATCH];
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const int i = threadIdx.x + (k0 + j) * THREADS;
+            const int ry = i / RWMAX, rx = i % RWMAX;
+            in[j] = (k0 + j < CELLS) && ry < G::RH && rx < G::RW;
+            ok[j] = false;
+            off[j] = 0;
+            fa[j] = fb[j] = 0.f;
+            if (in[j]) {
+                const int iy = mirror_idx(y0 - G::R + ry, h), ix = mirror_idx(x0 - G::R + rx, w);
+                const float X = (float)(ix + 1), Y = (float)(iy + 1);
+                float xs, ys;
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    // h * (l+1, k+1, 1), then x / x.z - 1 (kernels.cu:39-40), no contraction
+                    const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
+                    const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
+                    const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
+                    xs = q0 / q2 - 1.f;
+                    ys = q1 / q2 - 1.f;
+                } else {
+                    const float q0 = fmaf(Hm[0], X, fmaf(Hm[1], Y, Hm[2]));
+                    const float q1 = fmaf(Hm[3], X, fmaf(Hm[4], Y, Hm[5]));
+                    const float q2 = fmaf(Hm[6], X, fmaf(Hm[7], Y, Hm[8]));
+                    float rz;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rz) : "f"(q2));
+                    xs = fmaf(q0, rz, -1.f);
+                    ys = fmaf(q1, rz, -1.f);
+                }
+                const float fx = floorf(xs), fy = floorf(ys);
+                // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
+                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= (float)(w - 1) && fy + 1.f <= (float)(h - 1);
+                if (ok[j]) {
+                    const int xi = (int)fx, yi = (int)fy;
+                    fa[j] = xs - (float)xi;
+                    fb[j] = ys - (float)yi;
+                    off[j] = yi * w + xi;
+                }
+            }
+        }
+        float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
+            if (ok[j]) {
+                const float *r0 = src + off[j];
+                d00[j] = ldg(r0);
+                d01[j] = ldg(r0 + 1);
+                d10[j] = ldg(r0 + w);
+                d11[j] = ldg(r0 + w + 1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            if (!in[j]) continue;
+            const int i = threadIdx.x + (k0 + j) * THREADS;
+            float v = 0.f;
+            if (ok[j]) {
+                const float a = fa[j], b = fb[j];
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    const float t1 = a * d01[j] + (1 - a) * d00[j];
+                    const float t2 = a * d11[j] + (1 - a) * d10[j];
+                    v = b * t2 + (1 - b) * t1;
+                } else {
+                    const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
+                    const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
+                    v = fmaf(b, t2 - t1, t1);
+                }
+            }
+            Wt[i / RWMAX][i % RWMAX] = v;
+        }
     }
 }
 
@@ -131,10 +172,10 @@ __device__ __forceinline__ void pass_a1(float (*Wt)[RWMAX], float (*CS)[TH][CSP]
     float wv[G::SROWS];
 #pragma unroll
     for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[8 * s + i][c];
+    if (MOM == MVS_MOMENTS_REFERENCE) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
-        if (MOM == MVS_MOMENTS_REFERENCE) {
+        for (int k = 0; k < 8; ++k) {
+            float s1 = 0.f, s2 = 0.f, s12 = 0.f;
             // windowed_mean_column_kernel on warped, warped^2 and ref*warped
 #pragma unroll
             for (int i = 0; i < WIN; ++i) {
@@ -146,18 +187,34 @@ __device__ __forceinline__ void pass_a1(float (*Wt)[RWMAX], float (*CS)[TH][CSP]
             s1 = s1 / (float)WIN;
             s2 = s2 / (float)WIN;
             s12 = s12 / (float)WIN;
-        } else {
-#pragma unroll
-            for (int i = 0; i < WIN; ++i) {
-                const float x = wv[k + i] - shift;
-                s1 += x;
-                s2 = fmaf(x, x, s2);
-                s12 = fmaf(refcol[k + i], x, s12);
-            }
+            CS[0][8 * s + k][c] = s1;
+            CS[1][8 * s + k][c] = s2;
+            CS[2][8 * s + k][c] = s12;
         }
-        CS[0][8 * s + k][c] = s1;
-        CS[1][8 * s + k][c] = s2;
-        CS[2][8 * s + k][c] = s12;
+    }
+    if (MOM != MVS_MOMENTS_REFERENCE) {
+        // sliding sums down the strip of shifted values
+#pragma unroll
+        for (int i = 0; i < G::SROWS; ++i) wv[i] -= shift;
+        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) {
+            s1 += wv[i];
+            s2 = fmaf(wv[i], wv[i], s2);
+            s12 = fmaf(refcol[i], wv[i], s12);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k > 0) {
+                const float xn = wv[k + WIN - 1], xo = wv[k - 1];
+                s1 = (s1 + xn) - xo;
+                s2 = fmaf(-xo, xo, fmaf(xn, xn, s2));
+                s12 = fmaf(-refcol[k - 1], xo, fmaf(refcol[k + WIN - 1], xn, s12));
+            }
+            CS[0][8 * s + k][c] = s1;
+            CS[1][8 * s + k][c] = s2;
+            CS[2][8 * s + k][c] = s12;
+        }
     }
 }
 
@@ -172,18 +229,40 @@ __device__ __forceinline__ void row_sums(float (*CS)[TH][CSP], int q, float *out
     float v[G::RUN + 2 * G::R];
 #pragma unroll
     for (int i = 0; i < G::RUN + 2 * G::R; ++i) v[i] = CS[q][y][g * G::RUN + i];
+    if (MOM == MVS_MOMENTS_REFERENCE) {
+        // windowed_mean_row_kernel: direct sum in window order, then / winsize
 #pragma unroll
-    for (int j = 0; j < G::RUN; ++j) {
+        for (int j = 0; j < G::RUN; ++j) {
+            float m = 0.f;
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) m = m + v[j + i];
+            out[j] = m / (float)WIN;
+        }
+    } else {
         float m = 0.f;
 #pragma unroll
-        for (int i = 0; i < WIN; ++i) m = m + v[j + i];
-        out[j] = (MOM == MVS_MOMENTS_REFERENCE) ? m / (float)WIN : m;
+        for (int i = 0; i < WIN; ++i) m += v[i];
+        out[0] = m;
+#pragma unroll
+        for (int j = 1; j < G::RUN; ++j) {
+            m = (m + v[j + WIN - 1]) - v[j - 1];
+            out[j] = m;
+        }
     }
+}
+
+// Rounding bound of n*Sxx - Sx^2 for the compensated sums, as a multiple of
+// Sxx: about 3 n eps per addition, with 2*WIN + 26 additions along the
+// column and row passes.  Windows at or below it count as flat.
+template <int WIN>
+__device__ __forceinline__ constexpr float flat_kappa()
+{
+    return 3.f * (float)(WIN * WIN) * (float)(2 * WIN + 26) * 5.9604645e-8f;
 }
 
 // Reference moments of the tile, once per CTA: in REFERENCE mode the mean and
 // the naive std (calculate_STD_kernel, kernels.cu:103-120) of the reference
-// window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2.
+// window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2 (0 if flat).
 template <int WIN, int MOM>
 __device__ void ref_moments(float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float *rm, float *rs)
 {
@@ -196,12 +275,12 @@ __device__ void ref_moments(float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shif
                 float s1 = 0.f, s2 = 0.f;
 #pragma unroll
                 for (int i = 0; i < WIN; ++i) {
-                    const float x = (MOM == MVS_MOMENTS_REFERENCE) ? Rt[8 * s + k + i][c]
-                                                                   : Rt[8 * s + k + i][c] - shift;
                     if (MOM == MVS_MOMENTS_REFERENCE) {
+                        const float x = Rt[8 * s + k + i][c];
                         s1 = s1 + x;
                         s2 = s2 + x * x;
                     } else {
+                        const float x = Rt[8 * s + k + i][c] - shift;
                         s1 += x;
                         s2 = fmaf(x, x, s2);
                     }
@@ -226,8 +305,9 @@ __device__ void ref_moments(float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shif
             rm[j] = m[j];
             rs[j] = var > 0 ? sqrtf(var) : 0.f;
         } else {
+            const float v = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
             rm[j] = m[j];
-            rs[j] = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
+            rs[j] = v > flat_kappa<WIN>() * q[j] ? v : 0.f;
         }
     }
     __syncthreads();
@@ -246,7 +326,7 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
         const float vx = fmaf(-s1, s1, n * s2);         // n^2 var_w
         const float cv = fmaf(-s1, rm, n * s12);        // n^2 cov
         const float thr = st * n;                        // std >= st  <=>  n^2 var >= (st n)^2
-        if (!(vx >= thr * thr) || !(rs >= thr * thr)) return 0.f;
+        if (!(vx >= thr * thr) || !(rs >= thr * thr) || !(vx > flat_kappa<WIN>() * s2)) return 0.f;
         return cv * rsqrtf(vx * rs);
     }
 }
@@ -256,6 +336,7 @@ struct __align__(16) Smem {
     float Wt[TH + 16][RWMAX];      // warped region (reference region at start)
     float CS[3][TH][CSP];          // column sums
     float Hm[9];
+    float red[THREADS / 32];
 };
 
 template <int WIN, int MOM>
@@ -268,6 +349,28 @@ __device__ __forceinline__ void load_ref_region(Smem &S, const float *__restrict
         if (rx >= G::RW) continue;
         S.Wt[ry][rx] = ldg(ref + (size_t)mirror_idx(y0 - G::R + ry, h) * w + mirror_idx(x0 - G::R + rx, w));
     }
+}
+
+// Shift of the compensated sums: the mean of the tile's reference region
+// (block reduction; every thread returns the same value).  0 in REFERENCE mode.
+template <int WIN, int MOM>
+__device__ __forceinline__ float tile_shift(Smem &S)
+{
+    using G = Geo<WIN>;
+    if (MOM == MVS_MOMENTS_REFERENCE) return 0.f;
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        if (rx < G::RW) acc += S.Wt[ry][rx];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    float t = 0.f;
+#pragma unroll
+    for (int k = 0; k < THREADS / 32; ++k) t += S.red[k];
+    return t / (float)(G::RH * G::RW);
 }
 
 // ---- per-view kernel -------------------------------------------------------------
@@ -285,7 +388,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
 
     load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
     __syncthreads();
-    const float shift = (MOM == MVS_MOMENTS_REFERENCE) ? 0.f : S.Wt[G::RH / 2][G::RW / 2];
+    const float shift = tile_shift<WIN, MOM>(S);
     float refcol[G::SROWS];
     {
         const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
@@ -363,7 +466,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs 
 
     load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
     __syncthreads();
-    const float shift = (MOM == MVS_MOMENTS_REFERENCE) ? 0.f : S.Wt[G::RH / 2][G::RW / 2];
+    const float shift = tile_shift<WIN, MOM>(S);
     float refcol[G::SROWS];
     {
         const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
@@ -476,24 +579,35 @@ __global__ void wta_finish_kernel(const unsigned long long *__restrict__ wta, co
     }
 }
 
-// WTA argmin over a stored BF16 cost volume [P][n]: the HBM-bound pass.  Each
-// thread owns 8 consecutive pixels (one 16-byte load per plane).
+// WTA argmin over a stored BF16 cost volume [P][n]: the HBM-bound pass.
+// A block owns 32 groups of 8 consecutive pixels; its 8 warps split the planes
+// into 8 contiguous slices, each lane reading one 16-byte group per plane (a
+// warp reads 512 contiguous bytes per plane).  The slices' minima are merged
+// in plane order through shared memory, so ties keep the earliest plane.
+constexpr int WTA_WARPS = 8;
+
 __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restrict__ cost, const float *__restrict__ depths,
                                                         int n, int P, float zfar, float *__restrict__ depth,
                                                         int32_t *__restrict__ labels, float *__restrict__ best)
 {
+    __shared__ float sc[WTA_WARPS][32][9];
+    __shared__ int sl[WTA_WARPS][32][9];
     const int n8 = n / 8;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n8; i += gridDim.x * blockDim.x) {
-        float bc[8];
-        int bl[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * 32 + lane;            // pixel group of this lane
+    const int per = (P + WTA_WARPS - 1) / WTA_WARPS;
+    const int p0 = wid * per, p1 = min(P, p0 + per);
+    float bc[8];
+    int bl[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            bc[j] = 3.f;
-            bl[j] = -1;
-        }
-        const uint4 *col = reinterpret_cast<const uint4 *>(cost) + i;
+    for (int j = 0; j < 8; ++j) {
+        bc[j] = 3.f;
+        bl[j] = -1;
+    }
+    if (g < n8) {
+        const uint4 *col = reinterpret_cast<const uint4 *>(cost) + g;
 #pragma unroll 4
-        for (int p = 0; p < P; ++p) {
+        for (int p = p0; p < p1; ++p) {
             const uint4 q = __ldcs(col + (size_t)p * n8);
             const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
@@ -505,14 +619,29 @@ __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restr
                 }
             }
         }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int k = 8 * i + j;
-            depth[k] = bl[j] >= 0 ? ldg(depths + bl[j]) : zfar;
-            if (labels) labels[k] = bl[j];
-            if (best) best[k] = bc[j];
-        }
     }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        sc[wid][lane][j] = bc[j];
+        sl[wid][lane][j] = bl[j];
+    }
+    __syncthreads();
+    // thread t finalises pixel j = t & 7 of group t >> 3
+    const int gl = threadIdx.x >> 3, j = threadIdx.x & 7;
+    const int gg = blockIdx.x * 32 + gl;
+    if (gg >= n8) return;
+    float c = 3.f;
+    int l = -1;
+#pragma unroll
+    for (int k = 0; k < WTA_WARPS; ++k)
+        if (sc[k][gl][j] < c) {
+            c = sc[k][gl][j];
+            l = sl[k][gl][j];
+        }
+    const int px = 8 * gg + j;
+    depth[px] = l >= 0 ? ldg(depths + l) : zfar;
+    if (labels) labels[px] = l;
+    if (best) best[px] = c;
 }
 
 // FP64 homographies: H = K (Rrel + trel e3^T / d) K^-1, H /= H22, for one
@@ -644,8 +773,8 @@ int sweep_wta_volume(const uint16_t *cost, const float *depths, int n, int P, fl
                      int32_t *labels, float *best, void *stream)
 {
     if (n % 8) return set_error(MVS_ERR_ARG, "WTA over a cost volume needs W*H divisible by 8");
-    const int grid = min(ceil_div(n / 8, 256), 16 * kSMs);
-    wta_volume_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(cost, depths, n, P, zfar, depth, labels, best);
+    wta_volume_kernel<<<ceil_div(n / 8, 32), 256, 0, (cudaStream_t)stream>>>(cost, depths, n, P, zfar, depth, labels,
+                                                                           best);
     return check_launch("wta_volume_kernel");
 }
 

@@ -399,8 +399,10 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
 
     const int cap = prm->max_iters > 0 ? prm->max_iters : prm->warps * prm->niters;
     const int check_every = prm->check_every > 0 ? prm->check_every : 10;
-    double *h_energy = nullptr;
-    if (prm->tol > 0) MVS_TRY_CUDA(cudaMallocHost(&h_energy, sizeof(double)));
+    // the energy is read back into pageable host memory: a synchronous 8-byte
+    // copy needs no pinned staging (allocating one per call costs milliseconds)
+    double host_energy = 0.0;
+    double *h_energy = &host_energy;
     int total = 0;
     double last_e = 0.0;
     bool done = false;
@@ -482,7 +484,6 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     }
     if (!rc && energy_out && prm->tol <= 0) {
         // energy of the final iterate for callers that ask for it
-        if (!h_energy) MVS_TRY_CUDA(cudaMallocHost(&h_energy, sizeof(double)));
         energy_kernel<<<kEnergyBlocks, EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
                                                    prm->lambda, prm->alpha0, prm->alpha1, L.partial);
         sum_partials_kernel<<<1, EB, 0, st>>>(L.partial, kEnergyBlocks, L.energy);
@@ -491,7 +492,6 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         if (e != cudaSuccess) rc = set_error(MVS_ERR_CUDA, "tgv2 energy: %s", cudaGetErrorString(e));
         last_e = *h_energy;
     }
-    if (h_energy) cudaFreeHost(h_energy);
     if (iters_out) *iters_out = total;
     if (energy_out) *energy_out = last_e;
     return rc;

@@ -76,14 +76,18 @@ def test_reference_arithmetic_bit_exact_vs_reference(cuda, golden, name):
     np.testing.assert_array_equal(r["depth"], g["depth"])
 
 
-def assert_label_parity(lab, best, ref_lab, ref_best, same_min=0.999):
+def assert_label_parity(lab, best, ref_lab, ref_best, same_min=0.999, tie_tol=1e-3, weak=0.5):
     """Labels identical on >= same_min of the pixels; elsewhere within one plane, except
-    ties: where the labels are further apart the two best NCCs agree to 1e-4."""
+    where the match is a tie (the two best NCCs agree to tie_tol) or too weak to enter the
+    depthmap (both best NCCs <= the NCC threshold, `weak`)."""
     d = np.abs(lab.astype(np.int64) - ref_lab.astype(np.int64))
     same = float(np.mean(d == 0))
     far = d > 1
     assert same >= same_min, (same, float(np.mean(far)))
-    assert np.all(np.abs(best[far] - ref_best[far]) < 1e-4), float(np.mean(far))
+    tie = np.abs(best - ref_best) < tie_tol
+    unused = np.maximum(best, ref_best) <= weak
+    assert np.all((tie | unused)[far]), (float(np.mean(far)), best[far & ~(tie | unused)][:8],
+                                         ref_best[far & ~(tie | unused)][:8])
     return same
 
 
