@@ -109,7 +109,8 @@ int mvs_sweep(const mvs_sweep_desc *desc, const float *d_ref, const float *d_src
               void *d_workspace, size_t workspace_bytes, void *stream);
 
 /* Winner-take-all argmin over a stored BF16 cost volume (d_cost:
- * n_planes * n_pixels, as mvs_sweep writes it; n_pixels divisible by 8).
+ * n_planes * n_pixels, as mvs_sweep writes it: costs >= 0; n_pixels divisible
+ * by 8; n_planes <= 65535).
  * Writes the winning plane's depth (zfar if none), optional label and cost. */
 int mvs_sweep_wta_volume(const uint16_t *d_cost, const float *d_depths, int32_t n_pixels, int32_t n_planes,
                          float zfar, float *d_depth, int32_t *d_labels, float *d_best, void *stream);

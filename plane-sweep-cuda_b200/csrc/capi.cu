@@ -190,6 +190,7 @@ int mvs_sweep_wta_volume(const uint16_t *cost, const float *depths, int32_t n_pi
 {
     clear_error();
     if (!cost || !depths || !depth || n_pixels <= 0 || n_planes <= 0) return set_error(MVS_ERR_ARG, "bad argument");
+    if (n_planes > 65535) return set_error(MVS_ERR_ARG, "at most 65535 planes in a cost volume");
     return sweep_wta_volume(cost, depths, n_pixels, n_planes, zfar, depth, labels, best, stream);
 }
 

@@ -71,32 +71,53 @@ struct SweepArgs {
 
 // ---- pass A0: warp the region into shared memory ------------------------------
 
-// Cells are processed in batches: all coordinates of a batch first, then all
-// of its gathers, then the interpolation, so that each thread keeps several
-// independent L1/L2 gathers in flight.
-template <int WIN, int MOM>
-__device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h, int x0,
-                                        int y0, const float *Hm)
+// Thread t always owns region column rx = t & 63 and rows (t >> 6) + 4k, so its
+// pixel column X and its CELLS pixel rows Y_k (mirrored at the image border)
+// are fixed for the whole CTA: `Ycol` holds them, and per plane only the
+// X-dependent part of H*(X, Y, 1) is formed once (COMPENSATED; the REFERENCE
+// path keeps the reference's dot-product order).  Cells are processed in
+// batches -- coordinates, then all gathers, then the interpolation -- so each
+// thread keeps several independent L1/L2 gathers in flight.
+template <int WIN>
+struct A0Cells {
+    static constexpr int CELLS = (Geo<WIN>::RH * RWMAX + THREADS - 1) / THREADS;
+};
+
+template <int WIN>
+__device__ __forceinline__ void a0_setup(int w, int h, int x0, int y0, float &Xcol, float *Ycol)
 {
     using G = Geo<WIN>;
-    constexpr int CELLS = (G::RH * RWMAX + THREADS - 1) / THREADS;
+    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
+    Xcol = (float)(mirror_idx(x0 - G::R + rx, w) + 1);
+#pragma unroll
+    for (int k = 0; k < A0Cells<WIN>::CELLS; ++k) Ycol[k] = (float)(mirror_idx(y0 - G::R + rb + 4 * k, h) + 1);
+}
+
+template <int WIN, int MOM>
+__device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h,
+                                        const float *Hm, float X, const float *Ycol)
+{
+    using G = Geo<WIN>;
+    constexpr int CELLS = A0Cells<WIN>::CELLS;
     constexpr int BATCH = 4;
+    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
+    if (rx >= G::RW) return;
+    // X-dependent part of the homography, once per plane
+    const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
+    const float wm1 = (float)(w - 1), hm1 = (float)(h - 1);
 #pragma unroll
     for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
         float fa[BATCH], fb[BATCH];
         int off[BATCH];
-        bool in[BATCH], ok[BATCH];
+        bool ok[BATCH];
 #pragma unroll
         for (int j = 0; j < BATCH; ++j) {
-            const int i = threadIdx.x + (k0 + j) * THREADS;
-            const int ry = i / RWMAX, rx = i % RWMAX;
-            in[j] = (k0 + j < CELLS) && ry < G::RH && rx < G::RW;
+            const int k = k0 + j;
             ok[j] = false;
             off[j] = 0;
             fa[j] = fb[j] = 0.f;
-            if (in[j]) {
-                const int iy = mirror_idx(y0 - G::R + ry, h), ix = mirror_idx(x0 - G::R + rx, w);
-                const float X = (float)(ix + 1), Y = (float)(iy + 1);
+            if (k < CELLS && rb + 4 * k < G::RH) {
+                const float Y = Ycol[k];
                 float xs, ys;
                 if (MOM == MVS_MOMENTS_REFERENCE) {
                     // h * (l+1, k+1, 1), then x / x.z - 1 (kernels.cu:39-40), no contraction
@@ -106,9 +127,7 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
                     xs = q0 / q2 - 1.f;
                     ys = q1 / q2 - 1.f;
                 } else {
-                    const float q0 = fmaf(Hm[0], X, fmaf(Hm[1], Y, Hm[2]));
-                    const float q1 = fmaf(Hm[3], X, fmaf(Hm[4], Y, Hm[5]));
-                    const float q2 = fmaf(Hm[6], X, fmaf(Hm[7], Y, Hm[8]));
+                    const float q0 = fmaf(Hm[1], Y, a0), q1 = fmaf(Hm[4], Y, a1), q2 = fmaf(Hm[7], Y, a2);
                     float rz;
                     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rz) : "f"(q2));
                     xs = fmaf(q0, rz, -1.f);
@@ -116,11 +135,11 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
                 }
                 const float fx = floorf(xs), fy = floorf(ys);
                 // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
-                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= (float)(w - 1) && fy + 1.f <= (float)(h - 1);
+                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= wm1 && fy + 1.f <= hm1;
                 if (ok[j]) {
                     const int xi = (int)fx, yi = (int)fy;
-                    fa[j] = xs - (float)xi;
-                    fb[j] = ys - (float)yi;
+                    fa[j] = xs - fx;
+                    fb[j] = ys - fy;
                     off[j] = yi * w + xi;
                 }
             }
@@ -139,8 +158,8 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
         }
 #pragma unroll
         for (int j = 0; j < BATCH; ++j) {
-            if (!in[j]) continue;
-            const int i = threadIdx.x + (k0 + j) * THREADS;
+            const int k = k0 + j;
+            if (k >= CELLS || rb + 4 * k >= G::RH) continue;
             float v = 0.f;
             if (ok[j]) {
                 const float a = fa[j], b = fb[j];
@@ -154,7 +173,7 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
                     v = fmaf(b, t2 - t1, t1);
                 }
             }
-            Wt[i / RWMAX][i % RWMAX] = v;
+            Wt[rb + 4 * k][rx] = v;
         }
     }
 }
@@ -400,6 +419,8 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
     }
     float rm[G::RUN], rs[G::RUN];
     ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+    float Xcol, Ycol[A0Cells<WIN>::CELLS];
+    a0_setup<WIN>(w, h, x0, y0, Xcol, Ycol);
 
     float best[G::RUN];
     int lab[G::RUN];
@@ -416,7 +437,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
         float Hm[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-        pass_a0<WIN, MOM>(S.Wt, src, w, h, x0, y0, Hm);
+        pass_a0<WIN, MOM>(S.Wt, src, w, h, Hm, Xcol, Ycol);
         __syncthreads();
         pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
         __syncthreads();
@@ -478,6 +499,8 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs 
     }
     float rm[G::RUN], rs[G::RUN];
     ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+    float Xcol, Ycol[A0Cells<WIN>::CELLS];
+    a0_setup<WIN>(w, h, x0, y0, Xcol, Ycol);
 
     const int y = y0 + (threadIdx.x >> 3);
     const int xb = x0 + (threadIdx.x & 7) * G::RUN;
@@ -500,7 +523,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs 
             float Hm[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-            pass_a0<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, x0, y0, Hm);
+            pass_a0<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, Hm, Xcol, Ycol);
             __syncthreads();
             pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
             __syncthreads();
@@ -513,7 +536,11 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs 
         }
 #pragma unroll
         for (int j = 0; j < G::RUN; ++j) {
-            const uint16_t cb = f2bf(fmaf(-acc[j], invV, 1.f));
+            // cost = 1 - mean NCC, clamped at 0 (rounding can push a perfect match
+            // below 0; the stored bf16 bits then order like unsigned integers)
+            float cf = fmaf(-acc[j], invV, 1.f);
+            cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
+            const uint16_t cb = f2bf(cf);
             const float c = bf2f(cb);
             const int x = xb + j;
             if (a.cost && y < h && x < w) a.cost[(size_t)p * n + (size_t)y * w + x] = cb;
@@ -590,20 +617,18 @@ __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restr
                                                         int n, int P, float zfar, float *__restrict__ depth,
                                                         int32_t *__restrict__ labels, float *__restrict__ best)
 {
-    __shared__ float sc[WTA_WARPS][32][9];
-    __shared__ int sl[WTA_WARPS][32][9];
+    __shared__ uint32_t sk[WTA_WARPS][32][9];
     const int n8 = n / 8;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int g = blockIdx.x * 32 + lane;            // pixel group of this lane
     const int per = (P + WTA_WARPS - 1) / WTA_WARPS;
     const int p0 = wid * per, p1 = min(P, p0 + per);
-    float bc[8];
-    int bl[8];
+    // (bf16 bits << 16 | plane): costs are >= 0, so their bf16 bits order like
+    // unsigned integers and a 32-bit min gives the lowest cost, then the
+    // earliest plane.
+    uint32_t key[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        bc[j] = 3.f;
-        bl[j] = -1;
-    }
+    for (int j = 0; j < 8; ++j) key[j] = 0xffffffffu;
     if (g < n8) {
         const uint4 *col = reinterpret_cast<const uint4 *>(cost) + g;
 #pragma unroll 4
@@ -611,33 +636,24 @@ __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restr
             const uint4 q = __ldcs(col + (size_t)p * n8);
             const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float c = bf2f((uint16_t)(wds[j >> 1] >> ((j & 1) * 16)));
-                if (c < bc[j]) {
-                    bc[j] = c;
-                    bl[j] = p;
-                }
+            for (int jj = 0; jj < 4; ++jj) {
+                key[2 * jj] = min(key[2 * jj], (wds[jj] << 16) | (uint32_t)p);
+                key[2 * jj + 1] = min(key[2 * jj + 1], (wds[jj] & 0xffff0000u) | (uint32_t)p);
             }
         }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        sc[wid][lane][j] = bc[j];
-        sl[wid][lane][j] = bl[j];
-    }
+    for (int j = 0; j < 8; ++j) sk[wid][lane][j] = key[j];
     __syncthreads();
     // thread t finalises pixel j = t & 7 of group t >> 3
     const int gl = threadIdx.x >> 3, j = threadIdx.x & 7;
     const int gg = blockIdx.x * 32 + gl;
     if (gg >= n8) return;
-    float c = 3.f;
-    int l = -1;
+    uint32_t kmin = 0xffffffffu;
 #pragma unroll
-    for (int k = 0; k < WTA_WARPS; ++k)
-        if (sc[k][gl][j] < c) {
-            c = sc[k][gl][j];
-            l = sl[k][gl][j];
-        }
+    for (int k = 0; k < WTA_WARPS; ++k) kmin = min(kmin, sk[k][gl][j]);
+    const int l = kmin == 0xffffffffu ? -1 : (int)(kmin & 0xffffu);
+    const float c = l >= 0 ? bf2f((uint16_t)(kmin >> 16)) : 3.f;
     const int px = 8 * gg + j;
     depth[px] = l >= 0 ? ldg(depths + l) : zfar;
     if (labels) labels[px] = l;
