@@ -108,6 +108,25 @@ int mvs_sweep(const mvs_sweep_desc *desc, const float *d_ref, const float *d_src
               const float *d_depths, float *d_depth, int32_t *d_labels, float *d_best, uint16_t *d_cost,
               void *d_workspace, size_t workspace_bytes, void *stream);
 
+/* mvs_sweep without caller workspace (no counterpart in the reference).
+ * For callers that cannot allocate device memory while they run -- host
+ * frameworks or plugin hosts that fix a library's device memory at start-up,
+ * real-time loops that cannot take cudaMalloc's latency and implicit
+ * synchronisation.  The sweep's scratch (one 64-bit word per pixel and view,
+ * or per pixel in the aggregated mode) lives in a fixed device array of
+ * mvs_sweep_noalloc_scratch_bytes() = 32 MiB inside the library, which every
+ * GPU that loads the library holds until the process exits; a larger sweep
+ * is rejected with MVS_ERR_ARG.  Nothing is allocated: the first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call outside any stream capture.  All calls share the one array,
+ * which keeps the last call's contents: calls that can overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the
+ * caller.  Arguments and outputs as mvs_sweep. */
+int mvs_sweep_noalloc(const mvs_sweep_desc *desc, const float *d_ref, const float *d_srcs, const float *d_H,
+                      const float *d_depths, float *d_depth, int32_t *d_labels, float *d_best, uint16_t *d_cost,
+                      void *stream);
+size_t mvs_sweep_noalloc_scratch_bytes(void);
+
 /* Winner-take-all argmin over a stored BF16 cost volume (d_cost:
  * n_planes * n_pixels, as mvs_sweep writes it: costs >= 0; n_pixels divisible
  * by 8; n_planes <= 65535).

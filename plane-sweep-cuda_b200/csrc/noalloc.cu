@@ -1,0 +1,86 @@
+// mvs_sweep_noalloc: the fused plane sweep with its scratch in a fixed,
+// library-owned device array instead of caller-allocated workspace.
+//
+// Some callers cannot allocate device memory when they run the sweep: host
+// frameworks and plugin hosts that hand a library all the device memory it may
+// use up front and forbid allocations afterwards, and real-time loops that
+// cannot afford cudaMalloc's latency and implicit device synchronisation.
+// They still pass their own inputs and outputs; the only memory the sweep
+// needs beyond those -- the per-pixel best-match words that the sweep kernel
+// and its epilogue exchange -- lives in `g_sweep_scratch` below.
+//
+// The array is a file-scope __device__ variable: every GPU that loads the
+// library holds its kNoAllocScratchBytes until the process exits.  Host code
+// must not pass the array's name to a kernel (on the host that name is a
+// stand-in, not a device address), so the device address is looked up once per
+// device with cudaGetSymbolAddress and cached.
+#include <mutex>
+
+#include "common.cuh"
+
+namespace mvs {
+
+int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode);
+int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
+                 float *depth, int32_t *labels, float *best, uint16_t *cost, unsigned long long *scratch,
+                 int n_chunks, void *stream);
+
+// 32 MiB: 4 Mi 64-bit words, one per pixel and source view in the per-view
+// mode (a 640x480 frame with up to 13 views) or one per pixel in the
+// aggregated mode (up to 4 Mi pixels).
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned long long g_sweep_scratch[kNoAllocScratchBytes / 8];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_lock;
+void *g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_sweep_scratch on the current device (looked up on the
+// first call for that device, with that device current).
+int scratch_address(void **out)
+{
+    int dev = 0;
+    MVS_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(MVS_ERR_ARG, "device %d out of range", dev);
+    std::lock_guard<std::mutex> g(g_lock);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
+        if (e != cudaSuccess)
+            return set_error(MVS_ERR_CUDA, "cudaGetSymbolAddress(sweep scratch): %s", cudaGetErrorString(e));
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return MVS_OK;
+}
+
+}  // namespace
+}  // namespace mvs
+
+extern "C" {
+
+size_t mvs_sweep_noalloc_scratch_bytes(void) { return mvs::kNoAllocScratchBytes; }
+
+int mvs_sweep_noalloc(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H,
+                      const float *depths, float *depth, int32_t *labels, float *best, uint16_t *cost, void *stream)
+{
+    using namespace mvs;
+    const size_t need = mvs_sweep_workspace_bytes(d);   // validates d; 0 if invalid
+    if (need == 0) return MVS_ERR_ARG;
+    if (need > kNoAllocScratchBytes)
+        return set_error(MVS_ERR_ARG,
+                         "mvs_sweep_noalloc: this sweep needs %zu bytes of scratch, the fixed array holds %zu "
+                         "(at most %zu pixel-view words); use mvs_sweep with a caller workspace",
+                         need, kNoAllocScratchBytes, kNoAllocScratchBytes / 8);
+    if (!ref || !srcs || !H || !depths || !depth) return set_error(MVS_ERR_ARG, "null input/output pointer");
+    if (d->mode == MVS_SWEEP_PER_VIEW && cost) return set_error(MVS_ERR_ARG, "cost volume is an aggregated-mode output");
+    void *scratch = nullptr;
+    if (int rc = scratch_address(&scratch)) return rc;
+    const int chunks = sweep_pick_chunks(d->window, d->width, d->height, d->n_views, d->n_planes, d->mode);
+    return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)scratch, chunks,
+                        stream);
+}
+
+}  // extern "C"

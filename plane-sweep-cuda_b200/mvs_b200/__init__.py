@@ -82,6 +82,8 @@ _sig("mvs_set_device", C.c_int, C.c_int)
 _sig("mvs_sweep_workspace_bytes", C.c_size_t, C.POINTER(SweepDesc))
 _sig("mvs_sweep_homographies", C.c_int, C.POINTER(SweepDesc), _D, _D, _D, _VP, _VP, _VP)
 _sig("mvs_sweep", C.c_int, C.POINTER(SweepDesc), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_size_t, _VP)
+_sig("mvs_sweep_noalloc", C.c_int, C.POINTER(SweepDesc), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP)
+_sig("mvs_sweep_noalloc_scratch_bytes", C.c_size_t)
 _sig("mvs_sweep_wta_volume", C.c_int, _VP, _VP, C.c_int32, C.c_int32, C.c_float, _VP, _VP, _VP, _VP)
 _sig("mvs_tgv2_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32, C.c_int32)
 _sig("mvs_tgv2_run", C.c_int, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _F, _F, _F, _F, C.POINTER(TGV2Params),
