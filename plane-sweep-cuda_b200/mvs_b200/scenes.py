@@ -170,8 +170,9 @@ class BoxScene:
             best = np.where(hit & (tnear < best), tnear, best)
         return best
 
-    def render(self, cam: Camera) -> tuple[np.ndarray, np.ndarray]:
-        """(intensity in [0,1], camera-z depth), both (H, W) float64."""
+    def render(self, cam: Camera, depth_only: bool = False) -> tuple[np.ndarray, np.ndarray]:
+        """(intensity in [0,1], camera-z depth), both (H, W) float64.  With
+        ``depth_only`` the texture lookup is skipped and intensity is None."""
         H, W = cam.height, cam.width
         xs, ys = np.meshgrid(np.arange(W, dtype=float), np.arange(H, dtype=float))
         pix = np.stack([xs, ys, np.ones_like(xs)], -1)
@@ -181,6 +182,8 @@ class BoxScene:
         s = self.cast(origin, dirs)
         miss = ~np.isfinite(s)
         s = np.where(miss, 50.0, s)
+        if depth_only:
+            return None, s
         pts = origin + dirs * s[..., None]
         inten = self.noise(pts)
         inten = np.where(miss, 0.5, inten)
@@ -328,14 +331,14 @@ class FusionInput:
 
 def fusion_sequence(seed: int, n_maps: int, width: int, height: int,
                     noise_frac: float = 0.01, outlier_frac: float = 0.02,
-                    cube: float = 5.0) -> FusionInput:
+                    cube: float = 5.0, fx: float | None = None) -> FusionInput:
     """Depthmaps of the box room along a smooth seeded trajectory.
 
     Gaussian depth noise with sigma = ``noise_frac`` * depth and
     ``outlier_frac`` of the pixels replaced by uniform random depths."""
     rng = np.random.default_rng(seed)
     sc = box_room(seed)
-    f = 0.75 * width
+    f = 0.75 * width if fx is None else fx
     K = intrinsics(f, f, (width - 1) / 2.0, (height - 1) / 2.0)
     depths, cams = [], []
     phase = rng.uniform(0, 2 * math.pi)
@@ -346,7 +349,7 @@ def fusion_sequence(seed: int, n_maps: int, width: int, height: int,
         target = np.array([0.3 * math.sin(a + 1.0), 0.3, 2.0])
         R, t = look_at(center, target)
         cam = Camera(K, R, t, width, height)
-        _, d = sc.render(cam)
+        _, d = sc.render(cam, depth_only=True)
         d = d * (1.0 + noise_frac * rng.standard_normal(d.shape))
         out = rng.random(d.shape) < outlier_frac
         d = np.where(out, rng.uniform(0.3, 6.0, d.shape), d)
