@@ -80,53 +80,55 @@ __device__ __forceinline__ void store_counts(uint16_t *__restrict__ hist, long i
     }
 }
 
+// Launch shape of the voxel kernels: a (32, 8, 1) block per 32 x 8 patch of
+// one z slice; grid (vw/32, vh/8, vd).  No index division anywhere.
+constexpr int VX = 32, VY = 8;
+
 template <int BINS>
-__global__ void __launch_bounds__(256) histogram_kernel(Dims D, uint16_t *__restrict__ hist,
-                                                        const float *__restrict__ depths, int w, int h, int nmaps,
-                                                        const float *__restrict__ cams, float threshold)
+__global__ void __launch_bounds__(VX *VY) histogram_kernel(Dims D, uint16_t *__restrict__ hist,
+                                                          const float *__restrict__ depths, int w, int h, int nmaps,
+                                                          const float *__restrict__ cams, float threshold)
 {
     constexpr int HS = HistStride<BINS>::value;
-    const long n = (long)D.vw * D.vh * D.vd;
+    const int x = blockIdx.x * VX + threadIdx.x, y = blockIdx.y * VY + threadIdx.y, z = blockIdx.z;
+    if (x >= D.vw || y >= D.vh) return;
+    const size_t i = (size_t)z * D.vw * D.vh + (size_t)y * D.vw + x;
     const float thresh = BINS == 2 ? 0.f : threshold;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x, y, z;
-        voxel_xyz(D, i, x, y, z);
-        // fusionData::worldCoords (fusion.h:360-364): (x + .5) / width in double
-        const float wx = (float)((x + .5) / D.vw), wy = (float)((y + .5) / D.vh), wz = (float)((z + .5) / D.vd);
-        const float cx = D.ax + D.sx * wx, cy = D.ay + D.sy * wy, cz = D.az + D.sz * wz;
-        uint32_t cnt[HS];
-        load_counts<HS>(hist, i, cnt);
-        for (int m = 0; m < nmaps; ++m) {
-            const float *K = cams + kMapCamFloats * m, *R = K + 9, *t = K + 18;
-            // c = R c + T; c = K c (fusion.cu:17-20)
-            const float r0 = ldg(R + 0) * cx + ldg(R + 1) * cy + ldg(R + 2) * cz + ldg(t + 0);
-            const float r1 = ldg(R + 3) * cx + ldg(R + 4) * cy + ldg(R + 5) * cz + ldg(t + 1);
-            const float r2 = ldg(R + 6) * cx + ldg(R + 7) * cy + ldg(R + 8) * cz + ldg(t + 2);
-            const float k0 = ldg(K + 0) * r0 + ldg(K + 1) * r1 + ldg(K + 2) * r2;
-            const float k1 = ldg(K + 3) * r0 + ldg(K + 4) * r1 + ldg(K + 5) * r2;
-            const float k2 = ldg(K + 6) * r0 + ldg(K + 7) * r1 + ldg(K + 8) * r2;
-            const float px = k0 / k2, py = k1 / k2;
-            if ((px < 0) || (px > w - 1) || (py < 0) || (py > h - 1)) continue;
-            const float flx = floorf(px), fly = floorf(py);
-            const int x0 = (int)fmaxf(flx, 0), y0 = (int)fmaxf(fly, 0);
-            const int x1 = (int)fminf(x0 + 1, w - 1), y1 = (int)fminf(y0 + 1, h - 1);
-            const float frx = px - flx, fry = py - fly;
-            const float *dm = depths + (size_t)m * w * h;
-            const float d00 = ldg(dm + x0 + y0 * w), d10 = ldg(dm + x1 + y0 * w);
-            const float d01 = ldg(dm + x0 + y1 * w), d11 = ldg(dm + x1 + y1 * w);
-            // bilinterp (dev_functions.h:33-38): lerp in y, then in x
-            const float l0 = d00 + fry * (d01 - d00), l1 = d10 + fry * (d11 - d10);
-            const float depth = l0 + frx * (l1 - l0);
-            const float sd = depth - k2;
-            int bin;
-            if (sd >= thresh) bin = BINS - 1;
-            else if (sd <= -thresh) bin = 0;
-            else bin = (int)(unsigned char)fminf(roundf((sd + thresh) / (2.f * thresh) * (BINS - 3) + 1), BINS - 2);
+    // fusionData::worldCoords (fusion.h:360-364): (x + .5) / width in double
+    const float wx = (float)((x + .5) / D.vw), wy = (float)((y + .5) / D.vh), wz = (float)((z + .5) / D.vd);
+    const float cx = D.ax + D.sx * wx, cy = D.ay + D.sy * wy, cz = D.az + D.sz * wz;
+    uint32_t cnt[HS];
+    load_counts<HS>(hist, (long)i, cnt);
+    for (int m = 0; m < nmaps; ++m) {
+        const float *K = cams + kMapCamFloats * m, *R = K + 9, *t = K + 18;
+        // c = R c + T; c = K c (fusion.cu:17-20)
+        const float r0 = ldg(R + 0) * cx + ldg(R + 1) * cy + ldg(R + 2) * cz + ldg(t + 0);
+        const float r1 = ldg(R + 3) * cx + ldg(R + 4) * cy + ldg(R + 5) * cz + ldg(t + 1);
+        const float r2 = ldg(R + 6) * cx + ldg(R + 7) * cy + ldg(R + 8) * cz + ldg(t + 2);
+        const float k0 = ldg(K + 0) * r0 + ldg(K + 1) * r1 + ldg(K + 2) * r2;
+        const float k1 = ldg(K + 3) * r0 + ldg(K + 4) * r1 + ldg(K + 5) * r2;
+        const float k2 = ldg(K + 6) * r0 + ldg(K + 7) * r1 + ldg(K + 8) * r2;
+        const float px = k0 / k2, py = k1 / k2;
+        if ((px < 0) || (px > w - 1) || (py < 0) || (py > h - 1)) continue;
+        const float flx = floorf(px), fly = floorf(py);
+        const int x0 = (int)fmaxf(flx, 0), y0 = (int)fmaxf(fly, 0);
+        const int x1 = (int)fminf(x0 + 1, w - 1), y1 = (int)fminf(y0 + 1, h - 1);
+        const float frx = px - flx, fry = py - fly;
+        const float *dm = depths + (size_t)m * w * h;
+        const float d00 = ldg(dm + x0 + y0 * w), d10 = ldg(dm + x1 + y0 * w);
+        const float d01 = ldg(dm + x0 + y1 * w), d11 = ldg(dm + x1 + y1 * w);
+        // bilinterp (dev_functions.h:33-38): lerp in y, then in x
+        const float l0 = d00 + fry * (d01 - d00), l1 = d10 + fry * (d11 - d10);
+        const float depth = l0 + frx * (l1 - l0);
+        const float sd = depth - k2;
+        int bin;
+        if (sd >= thresh) bin = BINS - 1;
+        else if (sd <= -thresh) bin = 0;
+        else bin = (int)(unsigned char)fminf(roundf((sd + thresh) / (2.f * thresh) * (BINS - 3) + 1), BINS - 2);
 #pragma unroll
-            for (int k = 0; k < BINS; ++k) cnt[k] += (bin == k);
-        }
-        store_counts<HS>(hist, i, cnt);
+        for (int k = 0; k < BINS; ++k) cnt[k] += (bin == k);
     }
+    store_counts<HS>(hist, (long)i, cnt);
 }
 
 // Bin centres (fusion.h:1041-1054).
@@ -181,52 +183,55 @@ __device__ __forceinline__ float prox_median(const uint32_t *cnt, float u, float
 }
 
 template <int BINS>
-__global__ void __launch_bounds__(256) update_u_kernel(Dims D, const uint16_t *__restrict__ hist, float *__restrict__ u,
-                                                       float *__restrict__ v, const float *__restrict__ p, double tau,
-                                                       double lambda)
+__global__ void __launch_bounds__(VX *VY) update_u_kernel(Dims D, const uint16_t *__restrict__ hist,
+                                                         float *__restrict__ u, float *__restrict__ v,
+                                                         const float *__restrict__ p, double tau, double lambda)
 {
     constexpr int HS = HistStride<BINS>::value;
-    const long n = (long)D.vw * D.vh * D.vd;
+    const int x = blockIdx.x * VX + threadIdx.x, y = blockIdx.y * VY + threadIdx.y, z = blockIdx.z;
+    if (x >= D.vw || y >= D.vh) return;
+    const size_t sz = (size_t)D.vw * D.vh, n = sz * D.vd;
+    const size_t i = (size_t)z * sz + (size_t)y * D.vw + x;
     const float *px = p, *py = p + n, *pz = p + 2 * n;
     const float tl = (float)tau * (float)lambda;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x, y, z;
-        voxel_xyz(D, i, x, y, z);
-        // divPBwd (fusion.h:793-802)
-        float div = px[i] + py[i] + pz[i];
-        if (x > 0) div -= px[i - 1];
-        if (y > 0) div -= py[i - D.vw];
-        if (z > 0) div -= pz[i - (long)D.vw * D.vh];
-        const double un = u[i];
-        const double uu = un - tau * (-(double)div);
-        uint32_t cnt[HS];
-        load_counts<HS>(hist, i, cnt);
-        const float m = prox_median<BINS>(cnt, (float)uu, tl);
-        u[i] = m;
-        v[i] = (float)((double)(2 * m) - un);
-    }
+    // divPBwd (fusion.h:793-802)
+    float div = px[i] + py[i] + pz[i];
+    if (x > 0) div -= px[i - 1];
+    if (y > 0) div -= py[i - D.vw];
+    if (z > 0) div -= pz[i - sz];
+    const double un = u[i];
+    const double uu = un - tau * (-(double)div);
+    uint32_t cnt[HS];
+    load_counts<HS>(hist, (long)i, cnt);
+    const float m = prox_median<BINS>(cnt, (float)uu, tl);
+    u[i] = m;
+    v[i] = (float)((double)(2 * m) - un);
 }
 
-__global__ void __launch_bounds__(256) update_p_kernel(Dims D, const float *__restrict__ v, float *__restrict__ p,
-                                                       float sigma)
+__global__ void __launch_bounds__(VX *VY) update_p_kernel(Dims D, const float *__restrict__ v, float *__restrict__ p,
+                                                         float sigma)
 {
-    const long n = (long)D.vw * D.vh * D.vd;
+    const int x = blockIdx.x * VX + threadIdx.x, y = blockIdx.y * VY + threadIdx.y, z = blockIdx.z;
+    if (x >= D.vw || y >= D.vh) return;
+    const size_t sz = (size_t)D.vw * D.vh, n = sz * D.vd;
+    const size_t i = (size_t)z * sz + (size_t)y * D.vw + x;
     float *px = p, *py = p + n, *pz = p + 2 * n;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x, y, z;
-        voxel_xyz(D, i, x, y, z);
-        const float vi = v[i];
-        // gradVFwd (fusion.h:773-781): zero at the far faces
-        const float gx = x < D.vw - 1 ? v[i + 1] - vi : 0.f;
-        const float gy = y < D.vh - 1 ? v[i + D.vw] - vi : 0.f;
-        const float gz = z < D.vd - 1 ? v[i + (long)D.vw * D.vh] - vi : 0.f;
-        const float qx = px[i] + sigma * gx, qy = py[i] + sigma * gy, qz = pz[i] + sigma * gz;
-        // projectUnitBall (fusion.h:866-870)
-        const float d = fmaxf(1.f, sqrtf(qx * qx + qy * qy + qz * qz));
-        px[i] = qx / d;
-        py[i] = qy / d;
-        pz[i] = qz / d;
+    const float vi = v[i];
+    // gradVFwd (fusion.h:773-781): zero at the far faces
+    const float gx = x < D.vw - 1 ? v[i + 1] - vi : 0.f;
+    const float gy = y < D.vh - 1 ? v[i + D.vw] - vi : 0.f;
+    const float gz = z < D.vd - 1 ? v[i + sz] - vi : 0.f;
+    float qx = px[i] + sigma * gx, qy = py[i] + sigma * gy, qz = pz[i] + sigma * gz;
+    // projectUnitBall (fusion.h:866-870); dividing by exactly 1 is the identity
+    const float d = fmaxf(1.f, sqrtf(qx * qx + qy * qy + qz * qz));
+    if (d != 1.f) {
+        qx = qx / d;
+        qy = qy / d;
+        qz = qz / d;
     }
+    px[i] = qx;
+    py[i] = qy;
+    pz[i] = qz;
 }
 
 __global__ void extract_count_kernel(const float *__restrict__ u, long n, float lo, float hi,
@@ -298,7 +303,7 @@ Dims dims_of(int vw, int vh, int vd, const float *a, const float *b)
 
 const float kZero3[3] = {0.f, 0.f, 0.f};
 
-int grid_for(long n) { return (int)std::min<long>((n + 255) / 256, 16L * kSMs); }
+dim3 voxel_grid(int vw, int vh, int vd) { return dim3((vw + VX - 1) / VX, (vh + VY - 1) / VY, vd); }
 
 }  // namespace
 
@@ -310,9 +315,8 @@ int fusion_histogram(int vw, int vh, int vd, int bins, const float *a, const flo
                      const float *depths, int nmaps, int w, int h, const float *d_cams, float thr, cudaStream_t st)
 {
     const Dims D = dims_of(vw, vh, vd, a, b);
-    const long n = (long)vw * vh * vd;
     switch (bins) {
-#define H(N) case N: histogram_kernel<N><<<grid_for(n), 256, 0, st>>>(D, hist, depths, w, h, nmaps, d_cams, thr); break;
+#define H(N) case N: histogram_kernel<N><<<voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st>>>(D, hist, depths, w, h, nmaps, d_cams, thr); break;
         MVS_BINS(H)
 #undef H
     default: return set_error(MVS_ERR_ARG, "bins %d not supported (2..10)", bins);
@@ -324,9 +328,8 @@ int fusion_update_u(int vw, int vh, int vd, int bins, const uint16_t *hist, floa
                     double tau, double lambda, cudaStream_t st)
 {
     const Dims D = dims_of(vw, vh, vd, kZero3, kZero3);
-    const long n = (long)vw * vh * vd;
     switch (bins) {
-#define U(N) case N: update_u_kernel<N><<<grid_for(n), 256, 0, st>>>(D, hist, u, v, p, tau, lambda); break;
+#define U(N) case N: update_u_kernel<N><<<voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st>>>(D, hist, u, v, p, tau, lambda); break;
         MVS_BINS(U)
 #undef U
     default: return set_error(MVS_ERR_ARG, "bins %d not supported (2..10)", bins);
@@ -337,8 +340,7 @@ int fusion_update_u(int vw, int vh, int vd, int bins, const uint16_t *hist, floa
 int fusion_update_p(int vw, int vh, int vd, const float *v, float *p, double sigma, cudaStream_t st)
 {
     const Dims D = dims_of(vw, vh, vd, kZero3, kZero3);
-    const long n = (long)vw * vh * vd;
-    update_p_kernel<<<grid_for(n), 256, 0, st>>>(D, v, p, (float)sigma);
+    update_p_kernel<<<voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st>>>(D, v, p, (float)sigma);
     return check_launch("fusion update_p_kernel");
 }
 

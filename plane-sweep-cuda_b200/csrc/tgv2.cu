@@ -165,7 +165,14 @@ struct IterBufs {
     float lambda, alpha0, alpha1, tau, sigma;
 };
 
-// One full TGV2 iteration (planesweep.cpp:485-509).
+// fmaxf(1.f, (float)sqrt(s)) of the reference's projections, without the
+// FP64 square root when s <= 1 (then the result is exactly 1).
+__device__ __forceinline__ double proj_norm(double s) { return s > 1.0 ? (double)fmaxf(1.f, (float)sqrt(s)) : 1.0; }
+
+// One full TGV2 iteration (planesweep.cpp:485-509).  The pixel's own operands
+// (r, It, Iu of every view, T, u, u0, v) are loaded before the shared-memory
+// phase so their latency overlaps the halo work.
+template <int VMAX>
 __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
 {
     __shared__ float sU[TY + 2][TX + 2], sVX[TY + 2][TX + 2], sVY[TY + 2][TX + 2];
@@ -174,6 +181,33 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     const int w = b.w, h = b.h;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    const bool own = x < w && y < h;
+    const int i = own ? y * w + x : 0;
+    const size_t n = (size_t)w * h;
+
+    // own-pixel operands, prefetched
+    float rv[VMAX], itv[VMAX], iuv[VMAX];
+    const int V = b.V;   // <= VMAX (the launch picks VMAX)
+#pragma unroll
+    for (int v = 0; v < VMAX; ++v) {
+        if (v < V && own) {
+            const size_t k = (size_t)v * n + i;
+            rv[v] = b.r[k];
+            itv[v] = b.It[k];
+            iuv[v] = b.Iu[k];
+        }
+    }
+    float t11 = 0.f, t12 = 0.f, t22 = 0.f, uold = 0.f, u0v = 0.f, u1xprev = 0.f, u1yprev = 0.f;
+    if (own) {
+        t11 = b.T11[i];
+        t12 = b.T12[i];
+        t22 = b.T22[i];
+        uold = b.u[i];
+        u0v = b.u0[i];
+        u1xprev = b.u1x[i];
+        u1yprev = b.u1y[i];
+    }
 
     // ubar, vbar on [x0-1, x0+TX] x [y0-1, y0+TY] (clamped; cells outside the
     // image are never read)
@@ -199,12 +233,12 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
         {
             const double xg = sU[ry][nx] - sU[ry][rx] - sVX[ry][rx];
             const double yg = sU[ny][rx] - sU[ry][rx] - sVY[ry][rx];
-            const double t11 = b.T11[j], t12 = b.T12[j], t22 = b.T22[j];
-            const double dx = (double)b.Px_in[j] + (double)a1s * (t11 * xg + t12 * yg);
-            const double dy = (double)b.Py_in[j] + (double)a1s * (t12 * xg + t22 * yg);
-            const double d = fmaxf(1.f, (float)sqrt(dx * dx + dy * dy));
-            sPx[ry][rx] = (float)(dx / d);
-            sPy[ry][rx] = (float)(dy / d);
+            const double c11 = b.T11[j], c12 = b.T12[j], c22 = b.T22[j];
+            const double dx = (double)b.Px_in[j] + (double)a1s * (c11 * xg + c12 * yg);
+            const double dy = (double)b.Py_in[j] + (double)a1s * (c12 * xg + c22 * yg);
+            const double d = proj_norm(dx * dx + dy * dy);
+            sPx[ry][rx] = (float)(d == 1.0 ? dx : dx / d);
+            sPy[ry][rx] = (float)(d == 1.0 ? dy : dy / d);
         }
         {
             const float dx_u1x = sVX[ry][nx] - sVX[ry][rx];
@@ -214,41 +248,37 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
             const double dx = b.Qx_in[j] + a0s * dx_u1x;
             const double dy = b.Qy_in[j] + a0s * dy_u1y;
             const double dz = b.Qz_in[j] + a0s * (dy_u1x + dx_u1y) / 2.0f;
-            const double d = fmaxf(1.f, (float)sqrt(dx * dx + dy * dy + dz * dz + dz * dz));
-            sQx[ry][rx] = (float)(dx / d);
-            sQy[ry][rx] = (float)(dy / d);
-            sQz[ry][rx] = (float)(dz / d);
+            const double d = proj_norm(dx * dx + dy * dy + dz * dz + dz * dz);
+            sQx[ry][rx] = (float)(d == 1.0 ? dx : dx / d);
+            sQy[ry][rx] = (float)(d == 1.0 ? dy : dy / d);
+            sQz[ry][rx] = (float)(d == 1.0 ? dz : dz / d);
         }
     }
     __syncthreads();
 
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= w || y >= h) return;
-    const int i = y * w + x;
+    if (!own) return;
     const int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
-    const size_t n = (size_t)w * h;
 
     // r and prodsum (TGV2_updateR_kernel, TGV2_kernels.cu:87-105), views in order
-    const float uold = b.u[i], du = uold - b.u0[i];
+    const float du = uold - u0v;
     const float sl = b.sigma * b.lambda;
     float prodsum = 0.f;
-    for (int v = 0; v < b.V; ++v) {
-        const size_t k = (size_t)v * n + i;
-        const float iu = b.Iu[k];
-        float r = b.r[k] + sl * (b.It[k] + du * iu);
-        r = r / fmaxf(1.f, fabsf(r));
-        b.r[k] = r;
-        prodsum += r * iu;
+#pragma unroll
+    for (int v = 0; v < VMAX; ++v) {
+        if (v < V) {
+            float r = rv[v] + sl * (itv[v] + du * iuv[v]);
+            r = r / fmaxf(1.f, fabsf(r));
+            b.r[(size_t)v * n + i] = r;
+            prodsum += r * iuv[v];
+        }
     }
 
     // primal step (TGV2_updateU_tensor_weighed_kernel, TGV2_kernels.cu:300-338)
     const int xp = max(x - 1, 0), yp = max(y - 1, 0);
     const int lxp = lx - (x - xp), lyp = ly - (y - yp);
-    const float t11 = b.T11[i], t12 = b.T12[i], t22 = b.T22[i];
     const float c_px = sPx[ly][lx], c_py = sPy[ly][lx];
     const float xp_px = sPx[ly][lxp], yp_px = sPx[lyp][lx];
     const float xp_py = sPy[ly][lxp], yp_py = sPy[lyp][lx];
-    const float u1xprev = b.u1x[i], u1yprev = b.u1y[i];
     const float unew = uold - b.tau * (-b.alpha1 * (t11 * (c_px - xp_px) + t12 * (c_py - xp_py) +
                                                    t12 * (c_px - yp_px) + t22 * (c_py - yp_py)) +
                                        b.lambda * prodsum);
@@ -452,7 +482,10 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             ib.Qx_out = L.Qx[cur ^ 1];
             ib.Qy_out = L.Qy[cur ^ 1];
             ib.Qz_out = L.Qz[cur ^ 1];
-            iteration_kernel<<<gi, bi, 0, st>>>(ib);
+            if (V <= 4) iteration_kernel<4><<<gi, bi, 0, st>>>(ib);
+            else if (V <= 8) iteration_kernel<8><<<gi, bi, 0, st>>>(ib);
+            else if (V <= 16) iteration_kernel<16><<<gi, bi, 0, st>>>(ib);
+            else iteration_kernel<32><<<gi, bi, 0, st>>>(ib);
             cur ^= 1;
             ++total;
             if (prm->tol > 0 && (k + 1) % check_every == 0) {

@@ -88,9 +88,11 @@ __global__ void __launch_bounds__(TX *TY) tvl1_iteration_kernel(Bufs b)
         const double t11 = b.T11[j], t12 = b.T12[j], t22 = b.T22[j];
         const double dx = (double)b.Px_in[j] + (double)b.sigma_p * (t11 * x + t12 * y);
         const double dy = (double)b.Py_in[j] + (double)b.sigma_p * (t12 * x + t22 * y);
-        const double d = fmaxf(1.f, (float)sqrt(dx * dx + dy * dy));
-        sPx[ry][rx] = (float)(dx / d);
-        sPy[ry][rx] = (float)(dy / d);
+        // fmaxf(1, sqrt(s)) is exactly 1 for s <= 1, and dividing by 1 is the identity
+        const double s2 = dx * dx + dy * dy;
+        const double d = s2 > 1.0 ? (double)fmaxf(1.f, (float)sqrt(s2)) : 1.0;
+        sPx[ry][rx] = (float)(d == 1.0 ? dx : dx / d);
+        sPy[ry][rx] = (float)(d == 1.0 ? dy : dy / d);
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
