@@ -308,6 +308,24 @@ def main():
                   "tvl1_roofline": {"bound": "hbm", "achieved": tv_gbs, "peak": peaks()[0], "unit": "GB/s",
                                     "frac": tv_gbs / peaks()[0], "bytes_per_voxel_iteration": 68}}
 
+    if fusion is not None and rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # the reference's own fusion kernels on the host cores (oracle/_ref, OpenMP over
+        # blocks), on a bounded sample: a 96^3 volume of the same scene, all 40 maps, 4 iterations
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle as po
+        if po.ref_lib() is not None:
+            sdims = (96, 96, 96)
+            rv = po.RefVolume(7, sdims, fi.vol_min, fi.vol_max)
+            th = sum(rv.histogram(fi.depths[m], fK[m], fR[m], ft[m], 0.05) for m in range(40))
+            tt = 0.0
+            for _ in range(4):
+                tt += rv.update_u(0.1, 0.5) + rv.update_p(1.0)
+            nv = 96 ** 3
+            fusion["cpu_baseline"] = {"kind": "reference", "cores": os.cpu_count(),
+                                      "sample": "96^3 volume, the same 40 maps, 4 TV-L1 iterations",
+                                      "histogram_voxel_updates_per_s": nv * 40 / th,
+                                      "tvl1_voxel_iterations_per_s": nv * 4 / tt}
+
     # --- end to end through the PlaneSweep handle: host images in, host depthmap out ---
     ps = M.PlaneSweep()
     ps.setK(K1.astype(np.float32))
