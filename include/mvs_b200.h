@@ -166,6 +166,21 @@ int mvs_tgv2_run(int32_t width, int32_t height, int32_t n_views, const float *d_
                  int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
                  void *stream);
 
+/* Extension, no counterpart in the reference: TGV2 from a warm start.  The
+ * data term is linearised at d_u_lin (H*W; the plain run's start, e.g. the
+ * sweep's winner-take-all depth), so the energy is the plain run's; the
+ * primal starts at d_u (H*W, in/out) and d_v (2*H*W, vx then vy, in/out; NULL
+ * starts v at 0 and discards it).  dual_sigma > 0 starts p, q and r one dual
+ * step of that size from zero (0: at zero, as the plain run).  With d_u equal
+ * to d_u_lin, v = 0 and dual_sigma = 0 this is mvs_tgv2_run with
+ * u_from_input = 1.  Later linearisations (warps > 1) restart as the plain
+ * run does. */
+int mvs_tgv2_run_warm(int32_t width, int32_t height, int32_t n_views, const float *d_ref255, const float *d_srcs255,
+                      const float *h_K9, const float *h_invK9, const float *h_Rrel, const float *h_trel,
+                      const mvs_tgv2_params *params, const float *d_u_lin, float *d_u, float *d_v, double dual_sigma,
+                      int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
+                      void *stream);
+
 /* ---- TV-L1 depth denoise --------------------------------------------------
  * Replaces PlaneSweep::CudaDenoise's chain (planesweep.cpp:297-379):
  * Anisotropic_diffusion_tensor + denoising_TVL1_calculateP_tensor_weighed +
@@ -280,6 +295,78 @@ int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out);
 int mvs_ps_get_view_best(mvs_planesweep *ps, float *out);
 int mvs_ps_get_3d_coordinates(mvs_planesweep *ps, float *X, float *Y, float *Z); /* get3Dcoordinates */
 int mvs_ps_get_plane_count(mvs_planesweep *ps, int32_t *n);
+/* ---- synthetic scenes (no counterpart in the reference) -------------------
+ * Ray casts the seeded box scenes that stand in for the reference's datasets
+ * (ICL-NUIM, KITTI; reader.cpp, kitti_reader.cpp): an optional room seen
+ * from inside plus axis-aligned boxes, textured by value noise (a periodic
+ * lattice^3 table, `octaves` octaves from base_freq, each octave shifted by
+ * offsets[o]).  All FP64.  d_gray255 (may be NULL: depth only) receives
+ * 255 * intensity (0.5 where nothing is hit), d_depth the camera z (50 where
+ * nothing is hit).  h_invK9: inverse of the 0-based K; h_R9: world->camera
+ * rotation; h_center3: camera centre in the world. */
+typedef struct mvs_box_scene {
+    int32_t inside_room, n_boxes;      /* n_boxes <= 32 */
+    double room_min[3], room_max[3];
+    const double *h_boxes;             /* n_boxes x (min xyz, max xyz) */
+    const double *d_noise;             /* lattice^3 doubles, x slowest */
+    int32_t lattice, octaves;          /* octaves <= 8 */
+    double base_freq;
+    double offsets[8][3];
+} mvs_box_scene;
+
+int mvs_render_scene(const mvs_box_scene *scene, const double *h_invK9, const double *h_R9, const double *h_center3,
+                     int32_t width, int32_t height, float *d_gray255, float *d_depth, void *stream);
+
+/* ---- TGV2 warm-start network (no counterpart in the reference) -----------
+ * A 4-level U-Net (16/32/64/128 channels, 3x3 convolutions with ReLU, 2x2
+ * average pooling, nearest upsampling with skip concatenation, a 1x1 head)
+ * mapping the sweep's winner-take-all depth, its matching cost and the
+ * reference image to a prediction of the converged TGV2 primal (u, v) for
+ * mvs_tgv2_run_warm.  BF16 activations and weights on the tensor cores with
+ * FP32 accumulation; FP32 master weights and Adam.
+ *
+ * norm7 (may be NULL for the defaults {0.25, -1, 2, 1, 0.01, 1, 1}):
+ *   depth_scale, depth_shift  input channel 0 = depth * scale + shift
+ *   cost_clip                 input channel 1 = 1 - min(cost, clip)
+ *   u_scale, v_scale          u = wta + u_scale * head0, v = v_scale * head{1,2}
+ *   w_u, w_v                  loss = mean(w_u (u - u*)^2 + w_v |v - v*|^2)
+ * height and width must be multiples of 8.  Tensors are batch-major:
+ * d_wta, d_cost, d_ref255, d_u: batch*H*W; d_v: batch*2*H*W (vx then vy).
+ * Parameters are one FP32 array: per 3x3 layer W[cout][cin][3][3] then
+ * bias[cout] (mvs_unet_layer_info gives the offsets; layer 14 is the head,
+ * W[3][16] then bias[3]). */
+typedef struct mvs_unet mvs_unet;
+
+int mvs_unet_create(mvs_unet **out, int32_t batch, int32_t height, int32_t width, const float *norm7);
+int mvs_unet_destroy(mvs_unet *net);
+int64_t mvs_unet_param_count(const mvs_unet *net);
+int mvs_unet_layer_info(const mvs_unet *net, int32_t layer, int32_t *cin, int32_t *cout, int64_t *w_off,
+                        int64_t *b_off);
+int mvs_unet_set_params(mvs_unet *net, const float *h_params);            /* also resets Adam */
+int mvs_unet_get_params(mvs_unet *net, float *h_params, float *h_grads);  /* either may be NULL */
+int mvs_unet_forward(mvs_unet *net, const float *d_wta, const float *d_cost, const float *d_ref255, float *d_u,
+                     float *d_v, void *stream);
+/* gradients of the loss of the last forward against (d_u_target, d_v_target) */
+int mvs_unet_backward(mvs_unet *net, const float *d_u_target, const float *d_v_target, double *loss_out,
+                      void *stream);
+int mvs_unet_adam_step(mvs_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
+int mvs_unet_train_step(mvs_unet *net, const float *d_wta, const float *d_cost, const float *d_ref255,
+                        const float *d_u_target, const float *d_v_target, float lr, double *loss_out, void *stream);
+/* MVS_ERR_TIMEOUT if a bounded tensor-core wait gave up since the net was made */
+int mvs_unet_check(mvs_unet *net, void *stream);
+
+/* Single 3x3 layers (zero padding, NHWC bf16 bits, channels multiples of 16),
+ * for checks against a CPU restatement.  d_w: FP32 W[cout][cin][3][3];
+ * d_wpack: scratch of 2*9*cin*cout bf16; d_err: device int set on a timeout.
+ * backward: d_dw (9*cin*cout) and d_db (cout, may be NULL) are accumulated
+ * into; d_dx (may be NULL) = input gradient, times (x > 0) when mask_x. */
+int mvs_conv3x3_forward(const uint16_t *d_in, int32_t cin, const float *d_w, const float *d_bias, int32_t cout,
+                        int32_t batch, int32_t height, int32_t width, int32_t relu, uint16_t *d_out,
+                        uint16_t *d_wpack, int32_t *d_err, void *stream);
+int mvs_conv3x3_backward(const uint16_t *d_x, int32_t cin, const float *d_w, const uint16_t *d_dz, int32_t cout,
+                         int32_t batch, int32_t height, int32_t width, int32_t mask_x, uint16_t *d_dx, float *d_dw,
+                         float *d_db, uint16_t *d_wpack, int32_t *d_err, void *stream);
+
 /* Device time (ms) of the last run_algorithm / tgv / cuda_denoise call,
  * measured with CUDA events around the kernels only. */
 int mvs_ps_get_last_kernel_ms(mvs_planesweep *ps, float *ms);

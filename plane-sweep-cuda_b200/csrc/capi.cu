@@ -45,7 +45,8 @@ int sweep_homographies(const double *K, const double *invK, const double *Rrel, 
 size_t tgv2_workspace_bytes(int w, int h, int V);
 int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, const float *K9, const float *invK9,
              const float *Rrel, const float *trel, const mvs_tgv2_params *prm, int u_from_input, float u_init,
-             float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st);
+             float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st,
+             const TGV2Warm *warm = nullptr);
 // tvl1.cu
 size_t tvl1_workspace_bytes(int w, int h);
 int tvl1_run(int w, int h, const float *ref255, float *depth, float znear, float zfar, const mvs_tvl1_params *prm,
@@ -216,6 +217,27 @@ int mvs_tgv2_run(int32_t w, int32_t h, int32_t V, const float *ref255, const flo
     int it = 0;
     int rc = tgv2_run(w, h, V, ref255, srcs255, K9, invK9, Rrel, trel, prm, u_from_input, u_init, u, &it, energy_out,
                       ws, (cudaStream_t)stream);
+    if (iters_out) *iters_out = it;
+    return rc;
+}
+
+int mvs_tgv2_run_warm(int32_t w, int32_t h, int32_t V, const float *ref255, const float *srcs255, const float *K9,
+                      const float *invK9, const float *Rrel, const float *trel, const mvs_tgv2_params *prm,
+                      const float *u_lin, float *u, float *v, double dual_sigma, int32_t *iters_out,
+                      double *energy_out, void *ws, size_t ws_bytes, void *stream)
+{
+    clear_error();
+    if (w < 2 || h < 2 || V <= 0) return set_error(MVS_ERR_ARG, "bad size %dx%d, %d views", w, h, V);
+    if (!ref255 || !srcs255 || !K9 || !invK9 || !Rrel || !trel || !prm || !u || !u_lin)
+        return set_error(MVS_ERR_ARG, "null pointer");
+    if (prm->niters < 0 || prm->warps < 0) return set_error(MVS_ERR_ARG, "negative iteration count");
+    if (!(dual_sigma >= 0)) return set_error(MVS_ERR_ARG, "dual_sigma must be >= 0");
+    const size_t need = tgv2_workspace_bytes(w, h, V);
+    if (!ws || ws_bytes < need) return set_error(MVS_ERR_ARG, "workspace of %zu bytes needed", need);
+    TGV2Warm warm{u_lin, v, dual_sigma};
+    int it = 0;
+    int rc = tgv2_run(w, h, V, ref255, srcs255, K9, invK9, Rrel, trel, prm, 1, 0.f, u, &it, energy_out, ws,
+                      (cudaStream_t)stream, &warm);
     if (iters_out) *iters_out = it;
     return rc;
 }

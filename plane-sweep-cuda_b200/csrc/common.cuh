@@ -54,4 +54,14 @@ __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// Warm start of a TGV2 run: the data term is linearised at u_lin (first
+// linearisation) while the primal starts at the caller's u and at v (2 planes,
+// vx then vy; NULL = 0), which also receives the final v.  dual_sigma > 0
+// starts the dual variables one dual step of that size from zero.
+struct TGV2Warm {
+    const float *u_lin;
+    float *v;
+    double dual_sigma;
+};
+
 }  // namespace mvs

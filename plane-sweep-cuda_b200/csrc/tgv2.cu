@@ -86,6 +86,27 @@ __global__ void warp_init_kernel(int n, int V, const float *__restrict__ u, floa
     }
 }
 
+// Start of a warm-started linearisation: the data term is linearised at
+// u_lin while the primal starts at (u, v) -- e.g. a learned prediction of the
+// converged solution; dual variables and r start at zero.
+__global__ void warm_init_kernel(int n, int V, const float *__restrict__ u_lin, const float *__restrict__ u,
+                                 const float *__restrict__ vx, const float *__restrict__ vy, float *__restrict__ u0,
+                                 float *__restrict__ ubar, float *__restrict__ u1x, float *__restrict__ u1y,
+                                 float *__restrict__ u1xbar, float *__restrict__ u1ybar, float *__restrict__ Px,
+                                 float *__restrict__ Py, float *__restrict__ Qx, float *__restrict__ Qy,
+                                 float *__restrict__ Qz, float *__restrict__ r)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u0[i] = u_lin[i];
+        ubar[i] = u[i];
+        const float a = vx ? vx[i] : 0.f, c = vy ? vy[i] : 0.f;
+        u1x[i] = u1xbar[i] = a;
+        u1y[i] = u1ybar[i] = c;
+        Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
+        for (int k = 0; k < V; ++k) r[(size_t)k * n + i] = 0.f;
+    }
+}
+
 __global__ void fill_kernel(float *__restrict__ p, int n, float v)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
@@ -354,6 +375,52 @@ __global__ void sum_partials_kernel(const double *__restrict__ partial, int m, d
     }
 }
 
+// Dual start for a warm-started primal: one dual step of size sd from zero,
+// p = P(a1 sd T(grad u - v)), q = P(a0 sd e(v)), r_i = P(sd lambda (It_i +
+// (u - u0) Iu_i)), with the iteration's projections.  For a large sd this puts
+// each dual variable at the unit direction of its term, its value at the
+// saddle point wherever that term is non-zero.
+__global__ void dual_init_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
+                                 const float *__restrict__ T22, const float *__restrict__ It,
+                                 const float *__restrict__ Iu, const float *__restrict__ u0,
+                                 const float *__restrict__ u, const float *__restrict__ u1x,
+                                 const float *__restrict__ u1y, int w, int h, int V, float lambda, float alpha0,
+                                 float alpha1, float sd, float *__restrict__ Px, float *__restrict__ Py,
+                                 float *__restrict__ Qx, float *__restrict__ Qy, float *__restrict__ Qz,
+                                 float *__restrict__ r)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t n = (size_t)w * h;
+    const int i = y * w + x, xn = min(x + 1, w - 1), yn = min(y + 1, h - 1);
+    const int ix = y * w + xn, iy = yn * w + x;
+    {
+        const double xg = (double)u[ix] - u[i] - u1x[i];
+        const double yg = (double)u[iy] - u[i] - u1y[i];
+        const double s = (double)alpha1 * sd;
+        const double dx = s * (T11[i] * xg + T12[i] * yg), dy = s * (T12[i] * xg + T22[i] * yg);
+        const double d = proj_norm(dx * dx + dy * dy);
+        Px[i] = (float)(dx / d);
+        Py[i] = (float)(dy / d);
+    }
+    {
+        const double s = (double)alpha0 * sd;
+        const double dx = s * ((double)u1x[ix] - u1x[i]);
+        const double dy = s * ((double)u1y[iy] - u1y[i]);
+        const double dz = s * (((double)u1x[iy] - u1x[i]) + ((double)u1y[ix] - u1y[i])) / 2.0;
+        const double d = proj_norm(dx * dx + dy * dy + dz * dz + dz * dz);
+        Qx[i] = (float)(dx / d);
+        Qy[i] = (float)(dy / d);
+        Qz[i] = (float)(dz / d);
+    }
+    const float du = u[i] - u0[i];
+    for (int v = 0; v < V; ++v) {
+        const size_t k = (size_t)v * n + i;
+        float q = sd * lambda * (It[k] + du * Iu[k]);
+        r[k] = q / fmaxf(1.f, fabsf(q));
+    }
+}
+
 constexpr int kEnergyBlocks = 2 * kSMs;
 
 struct Layout {
@@ -406,7 +473,7 @@ size_t tgv2_workspace_bytes(int w, int h, int V) { return layout(nullptr, w, h, 
 
 int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, const float *K9, const float *invK9,
              const float *Rrel, const float *trel, const mvs_tgv2_params *prm, int u_from_input, float u_init,
-             float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st)
+             float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st, const TGV2Warm *warm)
 {
     if (V > kMaxViews) return set_error(MVS_ERR_ARG, "at most %d views", kMaxViews);
     Layout L = layout(ws, w, h, V);
@@ -435,6 +502,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     double *h_energy = &host_energy;
     int total = 0;
     double last_e = 0.0;
+    int energy_at = -1;   // iteration count at which last_e was evaluated
     bool done = false;
     IterBufs ib;
     ib.T11 = L.T11;
@@ -457,9 +525,18 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     ib.sigma = prm->sigma;
     const dim3 gi(ceil_div(w, TX), ceil_div(h, TY)), bi(TX, TY);
     for (int l = 0; l < prm->warps && !done; ++l) {
-        warp_init_kernel<<<eg, 256, 0, st>>>(n, V, u, L.u0, L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0],
-                                            L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0], L.r);
+        if (warm && l == 0)
+            warm_init_kernel<<<eg, 256, 0, st>>>(n, V, warm->u_lin, u, warm->v, warm->v ? warm->v + n : nullptr, L.u0,
+                                                L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0], L.Px[0], L.Py[0],
+                                                L.Qx[0], L.Qy[0], L.Qz[0], L.r);
+        else
+            warp_init_kernel<<<eg, 256, 0, st>>>(n, V, u, L.u0, L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0],
+                                                L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0], L.r);
         linearize_kernel<<<dim3(g2.x, g2.y, V), b2, 0, st>>>(cams, srcs255, L.ref01, L.u0, w, h, L.It, L.Iu);
+        if (warm && l == 0 && warm->dual_sigma > 0)
+            dual_init_kernel<<<g2, b2, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
+                                               prm->lambda, prm->alpha0, prm->alpha1, (float)warm->dual_sigma,
+                                               L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0], L.r);
         rc = check_launch("tgv2 linearisation");
         if (rc) break;
         int cur = 0;
@@ -500,6 +577,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
                     break;
                 }
                 last_e = *h_energy;
+                energy_at = total;
                 if (have_prev && fabs(prev - last_e) <= prm->tol * fabs(prev)) {
                     done = true;
                     break;
@@ -515,7 +593,12 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         if (!rc) rc = check_launch("tgv2 iteration");
         if (rc) break;
     }
-    if (!rc && energy_out && prm->tol <= 0) {
+    if (!rc && warm && warm->v) {
+        cudaMemcpyAsync(warm->v, L.u1x, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(warm->v + n, L.u1y, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        rc = check_launch("tgv2 v readout");
+    }
+    if (!rc && energy_out && energy_at != total) {
         // energy of the final iterate for callers that ask for it
         energy_kernel<<<kEnergyBlocks, EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
                                                    prm->lambda, prm->alpha0, prm->alpha1, L.partial);

@@ -18,6 +18,7 @@ Main entry points
 from __future__ import annotations
 
 import ctypes as C
+import math
 import pathlib
 
 import numpy as np
@@ -69,6 +70,13 @@ class TVL1Params(C.Structure):
                 ("theta", C.c_double), ("beta", C.c_double), ("gamma", C.c_double)]
 
 
+class BoxSceneDesc(C.Structure):
+    _fields_ = [("inside_room", C.c_int32), ("n_boxes", C.c_int32), ("room_min", C.c_double * 3),
+                ("room_max", C.c_double * 3), ("h_boxes", C.POINTER(C.c_double)), ("d_noise", C.c_void_p),
+                ("lattice", C.c_int32), ("octaves", C.c_int32), ("base_freq", C.c_double),
+                ("offsets", (C.c_double * 3) * 8)]
+
+
 def _sig(name, res, *args):
     f = getattr(_L, name)
     f.restype = res
@@ -88,6 +96,24 @@ _sig("mvs_sweep_wta_volume", C.c_int, _VP, _VP, C.c_int32, C.c_int32, C.c_float,
 _sig("mvs_tgv2_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32, C.c_int32)
 _sig("mvs_tgv2_run", C.c_int, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _F, _F, _F, _F, C.POINTER(TGV2Params),
      C.c_int32, C.c_float, _VP, _I32, _D, _VP, C.c_size_t, _VP)
+_sig("mvs_tgv2_run_warm", C.c_int, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _F, _F, _F, _F, C.POINTER(TGV2Params),
+     _VP, _VP, _VP, C.c_double, _I32, _D, _VP, C.c_size_t, _VP)
+_sig("mvs_render_scene", C.c_int, C.POINTER(BoxSceneDesc), _D, _D, _D, C.c_int32, C.c_int32, _VP, _VP, _VP)
+_sig("mvs_unet_create", C.c_int, C.POINTER(_VP), C.c_int32, C.c_int32, C.c_int32, _F)
+_sig("mvs_unet_destroy", C.c_int, _VP)
+_sig("mvs_unet_param_count", C.c_int64, _VP)
+_sig("mvs_unet_layer_info", C.c_int, _VP, C.c_int32, _I32, _I32, C.POINTER(C.c_int64), C.POINTER(C.c_int64))
+_sig("mvs_unet_set_params", C.c_int, _VP, _F)
+_sig("mvs_unet_get_params", C.c_int, _VP, _F, _F)
+_sig("mvs_unet_forward", C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP)
+_sig("mvs_unet_backward", C.c_int, _VP, _VP, _VP, _D, _VP)
+_sig("mvs_unet_adam_step", C.c_int, _VP, C.c_float, C.c_float, C.c_float, C.c_float, _VP)
+_sig("mvs_unet_train_step", C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, C.c_float, _D, _VP)
+_sig("mvs_unet_check", C.c_int, _VP, _VP)
+_sig("mvs_conv3x3_forward", C.c_int, _VP, C.c_int32, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+     C.c_int32, _VP, _VP, _VP, _VP)
+_sig("mvs_conv3x3_backward", C.c_int, _VP, C.c_int32, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+     C.c_int32, _VP, _VP, _VP, _VP, _VP, _VP)
 _sig("mvs_tvl1_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32)
 _sig("mvs_tvl1_denoise", C.c_int, C.c_int32, C.c_int32, _VP, _VP, C.c_float, C.c_float, C.POINTER(TVL1Params),
      _VP, C.c_size_t, _VP)
@@ -246,6 +272,31 @@ def tgv2_run(ref255, srcs255, K9, invK9, Rrel, trel, params, u, u_from_input=Fal
     return it.value, e.value
 
 
+def tgv2_run_warm(ref255, srcs255, K9, invK9, Rrel, trel, params, u_lin, u, v=None, dual_sigma=0.0,
+                  workspace=None, stream=None):
+    """TGV2 linearised at ``u_lin`` with the primal started at ``u`` (in/out)
+    and ``v`` ((2, H, W), in/out, or None for 0).  Returns (iterations,
+    final energy)."""
+    h, w = ref255.shape[-2:]
+    V = srcs255.shape[0]
+    it = C.c_int32(0)
+    e = C.c_double(0)
+    ws_bytes = 0 if workspace is None else workspace.numel() * workspace.element_size()
+    K9, invK9, Rrel, trel = (_f32(x) for x in (K9, invK9, Rrel, trel))
+    check(_L.mvs_tgv2_run_warm(w, h, V, _ptr(ref255), _ptr(srcs255), _fp(K9), _fp(invK9), _fp(Rrel), _fp(trel),
+                               C.byref(params), _ptr(u_lin), _ptr(u), _ptr(v), float(dual_sigma), C.byref(it),
+                               C.byref(e), _ptr(workspace), ws_bytes, _stream(stream)))
+    return it.value, e.value
+
+
+def render_scene(scene_desc, invK, R, center, width, height, gray255, depth, stream=None):
+    """Ray cast one view of a box scene on the device (see scenes.GpuRenderer)."""
+    invK, R, center = (np.ascontiguousarray(a, dtype=np.float64) for a in (invK, R, center))
+    check(_L.mvs_render_scene(C.byref(scene_desc), invK.ctypes.data_as(_D), R.ctypes.data_as(_D),
+                              center.ctypes.data_as(_D), width, height, _ptr(gray255), _ptr(depth),
+                              _stream(stream)))
+
+
 def tgv2_workspace_bytes(w, h, V):
     return int(_L.mvs_tgv2_workspace_bytes(w, h, V))
 
@@ -269,6 +320,109 @@ def compute3d(depth, invK9, Rr9, t3, X, Y, Z, stream=None):
     invK9, Rr9, t3 = (_f32(x) for x in (invK9, Rr9, t3))
     check(_L.mvs_compute3d(w, h, _ptr(depth), _fp(invK9), _fp(Rr9), _fp(t3), _ptr(X), _ptr(Y), _ptr(Z),
                            _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# TGV2 warm-start network
+# ---------------------------------------------------------------------------
+
+UNET_LAYERS = ((16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128),
+               (192, 64), (64, 64), (96, 32), (32, 32), (48, 16), (16, 16))
+UNET_DEFAULT_NORM = (0.25, -1.0, 2.0, 1.0, 0.01, 1.0, 1.0)
+
+
+class Unet:
+    """Handle on mvs_unet: forward, backward, Adam, parameters (FP32 host arrays)."""
+
+    def __init__(self, batch, height, width, norm=UNET_DEFAULT_NORM):
+        self.batch, self.height, self.width = batch, height, width
+        self.norm = tuple(float(x) for x in norm)
+        nm = np.asarray(self.norm, np.float32)
+        h = _VP()
+        check(_L.mvs_unet_create(C.byref(h), batch, height, width, nm.ctypes.data_as(_F)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.mvs_unet_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def n_params(self):
+        return int(_L.mvs_unet_param_count(self._h))
+
+    def layer_info(self, layer):
+        ci, co = C.c_int32(), C.c_int32()
+        wo, bo = C.c_int64(), C.c_int64()
+        check(_L.mvs_unet_layer_info(self._h, layer, C.byref(ci), C.byref(co), C.byref(wo), C.byref(bo)))
+        return ci.value, co.value, wo.value, bo.value
+
+    def init_params(self, seed=0):
+        """He-normal 3x3 weights (input channels beyond the 3 features of the
+        first layer at zero), zero biases, a small random head."""
+        rng = np.random.default_rng(seed)
+        p = np.zeros(self.n_params, np.float32)
+        for l in range(len(UNET_LAYERS)):
+            ci, co, wo, bo = self.layer_info(l)
+            fan = 9 * (3 if l == 0 else ci)
+            w = rng.standard_normal((co, ci, 9)) * math.sqrt(2.0 / fan)
+            if l == 0:
+                w[:, 3:, :] = 0.0
+            p[wo:wo + co * ci * 9] = w.reshape(-1)
+        ci, co, wo, bo = self.layer_info(len(UNET_LAYERS))
+        p[wo:wo + 48] = rng.standard_normal(48) * 0.01
+        self.set_params(p)
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        check(_L.mvs_unet_set_params(self._h, p.ctypes.data_as(_F)))
+
+    def get_params(self, grads=False):
+        p = np.empty(self.n_params, np.float32)
+        g = np.empty(self.n_params, np.float32) if grads else None
+        check(_L.mvs_unet_get_params(self._h, p.ctypes.data_as(_F), None if g is None else g.ctypes.data_as(_F)))
+        return (p, g) if grads else p
+
+    def forward(self, wta, cost, ref255, u_out=None, v_out=None, stream=None):
+        check(_L.mvs_unet_forward(self._h, _ptr(wta), _ptr(cost), _ptr(ref255), _ptr(u_out), _ptr(v_out),
+                                  _stream(stream)))
+
+    def backward(self, u_target, v_target, stream=None):
+        loss = C.c_double(0)
+        check(_L.mvs_unet_backward(self._h, _ptr(u_target), _ptr(v_target), C.byref(loss), _stream(stream)))
+        return loss.value
+
+    def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        check(_L.mvs_unet_adam_step(self._h, lr, beta1, beta2, eps, _stream(stream)))
+
+    def train_step(self, wta, cost, ref255, u_target, v_target, lr, stream=None):
+        loss = C.c_double(0)
+        check(_L.mvs_unet_train_step(self._h, _ptr(wta), _ptr(cost), _ptr(ref255), _ptr(u_target), _ptr(v_target),
+                                     lr, C.byref(loss), _stream(stream)))
+        return loss.value
+
+    def check(self, stream=None):
+        check(_L.mvs_unet_check(self._h, _stream(stream)))
+
+
+def conv3x3_forward(x, w, bias, relu, out, wpack, err, stream=None):
+    """x (B, H, W, cin) bf16, w (cout, cin, 3, 3) float32 CUDA tensors."""
+    B, H, W, cin = x.shape
+    cout = w.shape[0]
+    check(_L.mvs_conv3x3_forward(_ptr(x), cin, _ptr(w), _ptr(bias), cout, B, H, W, int(relu), _ptr(out), _ptr(wpack),
+                                 _ptr(err), _stream(stream)))
+
+
+def conv3x3_backward(x, w, dz, mask_x, dx, dw, db, wpack, err, stream=None):
+    B, H, W, cin = x.shape
+    cout = w.shape[0]
+    check(_L.mvs_conv3x3_backward(_ptr(x), cin, _ptr(w), _ptr(dz), cout, B, H, W, int(mask_x), _ptr(dx), _ptr(dw),
+                                  _ptr(db), _ptr(wpack), _ptr(err), _stream(stream)))
 
 
 # ---------------------------------------------------------------------------

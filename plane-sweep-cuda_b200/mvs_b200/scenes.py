@@ -224,10 +224,10 @@ def intrinsics(fx: float, fy: float, cx: float, cy: float) -> np.ndarray:
     return np.array([[fx, 0.0, cx], [0.0, fy, cy], [0.0, 0.0, 1.0]])
 
 
-def make_frame(seed: int, width: int, height: int, K: np.ndarray,
-               n_src: int, baseline=(0.05, 0.05), rot_deg: float = 2.0,
-               scene: str = "room") -> Frame:
-    """Reference view + ``n_src`` source views around it.
+def frame_geometry(seed: int, width: int, height: int, K: np.ndarray,
+                   n_src: int, baseline=(0.05, 0.05), rot_deg: float = 2.0,
+                   scene: str = "room") -> tuple[BoxScene, Camera, list]:
+    """Scene, reference camera and source cameras of ``make_frame``.
 
     Source centres sit on an arc (a circle in the reference camera's x-y
     plane) with radius drawn from ``baseline`` (metres); each source camera
@@ -244,8 +244,7 @@ def make_frame(seed: int, width: int, height: int, K: np.ndarray,
         target = np.array([rng.uniform(-0.5, 0.5), 0.3, 20.0])
     R0, t0 = look_at(center, target)
     ref_cam = Camera(K.astype(float), R0, t0, width, height)
-    inten, depth = sc.render(ref_cam)
-    srcs, cams = [], []
+    cams = []
     for i in range(n_src):
         ang = 2.0 * math.pi * (i + rng.uniform(-0.2, 0.2)) / max(n_src, 1)
         r = rng.uniform(baseline[0], baseline[1])
@@ -254,12 +253,83 @@ def make_frame(seed: int, width: int, height: int, K: np.ndarray,
         d = np.radians(rng.uniform(-rot_deg, rot_deg, 3))
         Rs = rot_xyz(*d) @ R0
         ts = -Rs @ c
-        cam = Camera(K.astype(float), Rs, ts, width, height)
-        img, _ = sc.render(cam)
-        srcs.append((img * 255.0).astype(np.float32))
-        cams.append(cam)
+        cams.append(Camera(K.astype(float), Rs, ts, width, height))
+    return sc, ref_cam, cams
+
+
+def make_frame(seed: int, width: int, height: int, K: np.ndarray,
+               n_src: int, baseline=(0.05, 0.05), rot_deg: float = 2.0,
+               scene: str = "room") -> Frame:
+    """Reference view + ``n_src`` source views around it (see frame_geometry)."""
+    sc, ref_cam, cams = frame_geometry(seed, width, height, K, n_src, baseline, rot_deg, scene)
+    inten, depth = sc.render(ref_cam)
+    srcs = [(sc.render(cam)[0] * 255.0).astype(np.float32) for cam in cams]
     return Frame((inten * 255.0).astype(np.float32), srcs, ref_cam, cams,
                  depth.astype(np.float32))
+
+
+@dataclasses.dataclass
+class DeviceFrame:
+    """A frame rendered on the GPU: ``ref`` (H, W), ``srcs`` (V, H, W) in
+    0..255 and ``depth_gt`` (H, W) are float32 CUDA tensors."""
+    ref: object
+    srcs: object
+    ref_cam: Camera
+    src_cams: list
+    depth_gt: object
+
+
+class GpuRenderer:
+    """Renders BoxScene views with the library's ray caster (mvs_render_scene).
+
+    The same scene and cameras give the CPU caster's pixels up to rounding
+    order (FP64 throughout)."""
+
+    def __init__(self, device="cuda"):
+        self.device = device
+
+    def _desc(self, sc: BoxScene):
+        import torch
+        from . import BoxSceneDesc
+        table = torch.from_numpy(np.ascontiguousarray(sc.noise.table, dtype=np.float64)).to(self.device)
+        boxes = np.ascontiguousarray([np.concatenate([a, b]) for a, b in sc.boxes], dtype=np.float64).reshape(-1)
+        d = BoxSceneDesc()
+        d.inside_room = int(sc.inside_room)
+        d.n_boxes = len(sc.boxes)
+        for k in range(3):
+            d.room_min[k] = float(sc.room_min[k])
+            d.room_max[k] = float(sc.room_max[k])
+        import ctypes
+        d.h_boxes = boxes.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.d_noise = table.data_ptr()
+        d.lattice = sc.noise.lattice
+        d.octaves = sc.noise.octaves
+        d.base_freq = float(sc.noise.base_freq)
+        for o in range(sc.noise.octaves):
+            for k in range(3):
+                d.offsets[o][k] = float(sc.noise.offsets[o][k])
+        return d, (table, boxes)
+
+    def render(self, sc: BoxScene, cams, with_image=True):
+        """(gray255 (N, H, W) or None, depth (N, H, W)) for a list of cameras."""
+        import torch
+        from . import render_scene
+        desc, keep = self._desc(sc)
+        H, W = cams[0].height, cams[0].width
+        depth = torch.empty((len(cams), H, W), dtype=torch.float32, device=self.device)
+        gray = torch.empty_like(depth) if with_image else None
+        for k, cam in enumerate(cams):
+            render_scene(desc, np.linalg.inv(cam.K), cam.R, cam.center, W, H,
+                         None if gray is None else gray[k], depth[k])
+        torch.cuda.current_stream().synchronize()   # keeps the host table and boxes alive until done
+        del keep
+        return gray, depth
+
+    def frame(self, seed: int, width: int, height: int, K: np.ndarray, n_src: int,
+              baseline=(0.05, 0.05), rot_deg: float = 2.0, scene: str = "room") -> DeviceFrame:
+        sc, ref_cam, cams = frame_geometry(seed, width, height, K, n_src, baseline, rot_deg, scene)
+        gray, depth = self.render(sc, [ref_cam] + cams)
+        return DeviceFrame(gray[0], gray[1:].contiguous(), ref_cam, cams, depth[0])
 
 
 def inverse_depth_planes(znear: float, zfar: float, n: int) -> np.ndarray:

@@ -1,0 +1,291 @@
+"""Learned warm start for TGV2 refinement (no counterpart in the reference).
+
+The plain pipeline -- plane sweep (compensated moments, BF16 cost volume,
+winner-take-all) then TGV2 from the winner-take-all depth -- makes the
+training pairs: its inputs (winner-take-all depth, matching cost, reference
+image) and its converged TGV2 primal (u, v).  A U-Net (mvs_b200.Unet, tensor
+core kernels) learns the map; at run time its prediction starts TGV2
+(mvs_tgv2_run_warm) with the data term still linearised at the winner-take-all
+depth, so the warm and plain runs minimise the same energy and the plain run
+stays the judge (and the fallback) of the energy the warm start reaches.
+
+    python -m mvs_b200.warmstart train --scenes 2000 --out weights.npz
+
+Scenes are the seeded box rooms of mvs_b200.scenes at 640x480 with 8 source
+views (2-10 cm baselines), 256 inverse-depth planes over [0.4, 8] m and a 9x9
+window, rendered on the device.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import math
+import pathlib
+import time
+
+import numpy as np
+
+from . import hostmath as hm
+from . import scenes
+
+WEIGHTS = pathlib.Path(__file__).resolve().parent / "warmstart_weights.npz"
+
+
+@dataclasses.dataclass
+class FrameConfig:
+    width: int = 640
+    height: int = 480
+    n_src: int = 8
+    fx: float = 481.2
+    baseline: tuple = (0.02, 0.10)
+    znear: float = 0.4
+    zfar: float = 8.0
+    n_planes: int = 256
+    window: int = 9
+
+    @property
+    def K(self):
+        return scenes.intrinsics(self.fx, self.fx, (self.width - 1) / 2.0, (self.height - 1) / 2.0)
+
+
+def tgv_params(tol=1e-4, max_iters=500, check_every=10, **kw):
+    """TGV2 as the reference's PlaneSweep::TGV defaults (lambda 0.5, alpha0 2,
+    alpha1 1.5, tau 0.02, sigma 1, beta 0, gamma 1), one linearisation at the
+    start depth, stopped at relative energy change `tol` or `max_iters`."""
+    import mvs_b200 as M
+    return M.tgv2_params(niters=max_iters, warps=1, tol=tol, check_every=check_every, max_iters=max_iters, **kw)
+
+
+class Pipeline:
+    """Sweep + winner-take-all + TGV2 for frames of one configuration, with
+    its device buffers allocated once."""
+
+    def __init__(self, cfg: FrameConfig, device="cuda"):
+        import torch
+        import mvs_b200 as M
+        self.M, self.torch, self.cfg, self.dev = M, torch, cfg, device
+        W, H, V, P = cfg.width, cfg.height, cfg.n_src, cfg.n_planes
+        self.desc = M.sweep_desc(W, H, V, P, cfg.window, M.MOMENTS_COMPENSATED, M.SWEEP_AGGREGATED, 1e-4, 0.5,
+                                 cfg.zfar)
+        self.planes = torch.from_numpy(scenes.inverse_depth_planes(cfg.znear, cfg.zfar, P)).to(device)
+        self.H = torch.empty(V * P * 9, dtype=torch.float32, device=device)
+        self.depth = torch.empty((H, W), dtype=torch.float32, device=device)
+        self.labels = torch.empty((H, W), dtype=torch.int32, device=device)
+        self.best = torch.empty((H, W), dtype=torch.float32, device=device)
+        self.cost = torch.empty((P, H, W), dtype=torch.int16, device=device)
+        self.wsp = torch.empty(M.sweep_workspace_bytes(self.desc) // 8 + 1, dtype=torch.int64, device=device)
+        self.tws = torch.empty(M.tgv2_workspace_bytes(W, H, V) // 8 + 1, dtype=torch.int64, device=device)
+
+    def cams(self, frame):
+        rel = [self.M.relative_pose(frame.ref_cam.R, frame.ref_cam.t, c.R, c.t) for c in frame.src_cams]
+        K1 = frame.ref_cam.K_1based
+        Kf = np.float32(K1)
+        relf = [hm.relative_f32(frame.ref_cam.R, frame.ref_cam.t, c.R, c.t) for c in frame.src_cams]
+        return dict(rel=rel, K1=K1, Kf=Kf.reshape(9), iK=hm.inv3_f32(Kf).reshape(9),
+                    Rs=np.stack([r[0].reshape(9) for r in relf]), ts=np.stack([r[1] for r in relf]))
+
+    def sweep(self, frame, cams=None):
+        """Winner-take-all depth and its matching cost (views averaged, 1 - NCC)."""
+        M = self.M
+        c = cams or self.cams(frame)
+        M.sweep_homographies(self.desc, c["K1"], c["rel"], self.planes, self.H)
+        M.sweep(self.desc, frame.ref, frame.srcs, self.H, self.planes, self.depth, None, None, self.cost, self.wsp)
+        M.sweep_wta_volume(self.cost, self.planes, self.cfg.width * self.cfg.height, self.cfg.n_planes,
+                           self.cfg.zfar, self.depth, self.labels, self.best)
+        return self.depth, self.best
+
+    def tgv(self, frame, u_lin, u, v, prm, dual_sigma=0.0, cams=None):
+        """TGV2 linearised at u_lin from (u, v) (both in/out).  (iterations, energy)."""
+        c = cams or self.cams(frame)
+        return self.M.tgv2_run_warm(frame.ref, frame.srcs, c["Kf"], c["iK"], c["Rs"], c["ts"], prm, u_lin, u, v,
+                                    dual_sigma=dual_sigma, workspace=self.tws)
+
+
+def make_dataset(seeds, cfg: FrameConfig, target_iters: int, device="cuda", log=None):
+    """Training pairs for `seeds` on the device: inputs (wta, cost, ref) and the
+    TGV2 state after `target_iters` iterations from the winner-take-all depth
+    (u*, v*), stacked as (N, H, W) / (N, 2, H, W) float32 tensors."""
+    import torch
+    pipe = Pipeline(cfg, device)
+    rnd = scenes.GpuRenderer(device)
+    N, H, W = len(seeds), cfg.height, cfg.width
+    out = {k: torch.empty((N, H, W), dtype=torch.float32, device=device) for k in ("wta", "cost", "ref", "u")}
+    out["v"] = torch.empty((N, 2, H, W), dtype=torch.float32, device=device)
+    energies = np.zeros(N)
+    prm = tgv_params(tol=0.0, max_iters=target_iters)
+    t0 = time.time()
+    for k, s in enumerate(seeds):
+        fr = rnd.frame(int(s), W, H, cfg.K, cfg.n_src, baseline=cfg.baseline)
+        cams = pipe.cams(fr)
+        wta, best = pipe.sweep(fr, cams)
+        out["wta"][k].copy_(wta)
+        out["cost"][k].copy_(best)
+        out["ref"][k].copy_(fr.ref)
+        out["u"][k].copy_(wta)
+        out["v"][k].zero_()
+        _, energies[k] = pipe.tgv(fr, out["wta"][k], out["u"][k], out["v"][k], prm, cams=cams)
+        if log and (k + 1) % 100 == 0:
+            torch.cuda.synchronize()
+            log(f"dataset {k + 1}/{N} scenes, {time.time() - t0:.1f} s")
+    torch.cuda.synchronize()
+    out["energy"] = energies
+    return out
+
+
+def cosine_lr(step, total, lr0, lr1):
+    return lr1 + 0.5 * (lr0 - lr1) * (1 + math.cos(math.pi * min(step, total) / max(total, 1)))
+
+
+def train(data, steps, batch=4, lr0=1e-3, lr1=2e-5, seed=0, init=None, norm=None, log=None, device="cuda"):
+    """Adam on the device over random batches of `data`.  Returns (params, losses)."""
+    import torch
+    import mvs_b200 as M
+    N, H, W = data["wta"].shape
+    net = M.Unet(batch, H, W, norm or M.UNET_DEFAULT_NORM)
+    if init is None:
+        net.init_params(seed)
+    else:
+        net.set_params(init)
+    rng = np.random.default_rng(seed + 1)
+    bufs = {k: torch.empty((batch,) + tuple(data[k].shape[1:]), dtype=torch.float32, device=device)
+            for k in ("wta", "cost", "ref", "u", "v")}
+    losses = []
+    t0 = time.time()
+    for it in range(steps):
+        idx = torch.from_numpy(rng.choice(N, batch, replace=False)).to(device)
+        for k, b in bufs.items():
+            torch.index_select(data[k], 0, idx, out=b)
+        loss = net.train_step(bufs["wta"], bufs["cost"], bufs["ref"], bufs["u"], bufs["v"],
+                              cosine_lr(it, steps, lr0, lr1))
+        losses.append(loss)
+        if log and (it + 1) % 200 == 0:
+            log(f"step {it + 1}/{steps} loss {np.mean(losses[-200:]):.6g} ({time.time() - t0:.1f} s)")
+    net.check()
+    params = net.get_params()
+    net.close()
+    return params, np.asarray(losses)
+
+
+def save_weights(path, params, norm, meta):
+    np.savez_compressed(path, params=np.asarray(params, np.float32), norm=np.asarray(norm, np.float64),
+                        meta=np.array(repr(meta)))
+
+
+def load_weights(path=WEIGHTS):
+    with np.load(path) as z:
+        return z["params"], tuple(float(x) for x in z["norm"]), str(z["meta"])
+
+
+class WarmStart:
+    """Inference: U-Net prediction of (u, v) for one frame, then TGV2 from it."""
+
+    def __init__(self, cfg: FrameConfig, params=None, norm=None, device="cuda"):
+        import torch
+        import mvs_b200 as M
+        if params is None:
+            params, norm, _ = load_weights()
+        self.net = M.Unet(1, cfg.height, cfg.width, norm or M.UNET_DEFAULT_NORM)
+        self.net.set_params(params)
+        self.u = torch.empty((1, cfg.height, cfg.width), dtype=torch.float32, device=device)
+        self.v = torch.empty((1, 2, cfg.height, cfg.width), dtype=torch.float32, device=device)
+
+    def predict(self, wta, cost, ref):
+        self.net.forward(wta, cost, ref, self.u, self.v)
+        return self.u[0], self.v[0]
+
+
+def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=0.0, device="cuda", log=None):
+    """Plain TGV2 (from the winner-take-all depth) against the warm-started run
+    (network prediction, same linearisation and stopping rule) on `seeds`.
+
+    Per frame: device times (ms; the warm time includes the network), the
+    iteration counts, final energies, the iterations the warm run needs to go
+    below the plain run's final energy (checked every 10; None if it never
+    does within the cap) and the median |depth - ground truth| of each."""
+    import torch
+    import mvs_b200 as M
+    prm = prm or tgv_params()
+    pipe = Pipeline(cfg, device)
+    rnd = scenes.GpuRenderer(device)
+    ws = WarmStart(cfg, params, norm, device)
+    H, W = cfg.height, cfg.width
+    u = torch.empty((H, W), dtype=torch.float32, device=device)
+    v = torch.empty((2, H, W), dtype=torch.float32, device=device)
+    wta = torch.empty_like(u)
+    cost = torch.empty_like(u)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    rows = []
+    for s in seeds:
+        fr = rnd.frame(int(s), W, H, cfg.K, cfg.n_src, baseline=cfg.baseline)
+        cams = pipe.cams(fr)
+        d, c = pipe.sweep(fr, cams)
+        wta.copy_(d)
+        cost.copy_(c)
+        # plain
+        u.copy_(wta)
+        v.zero_()
+        a, b = ev(), ev()
+        a.record()
+        it_p, e_p = pipe.tgv(fr, wta, u, v, prm, cams=cams)
+        b.record()
+        torch.cuda.synchronize()
+        ms_p = a.elapsed_time(b)
+        err_p = float((u - fr.depth_gt).abs().median())
+        # warm: network + TGV2 from its prediction
+        a, b = ev(), ev()
+        a.record()
+        pu, pv = ws.predict(wta[None], cost[None], fr.ref[None])
+        u.copy_(pu)
+        v.copy_(pv)
+        it_w, e_w = pipe.tgv(fr, wta, u, v, prm, dual_sigma=dual_sigma, cams=cams)
+        b.record()
+        torch.cuda.synchronize()
+        ms_w = a.elapsed_time(b)
+        err_w = float((u - fr.depth_gt).abs().median())
+        # energy of the raw prediction and iterations to reach the plain energy
+        pu, pv = ws.predict(wta[None], cost[None], fr.ref[None])
+        u.copy_(pu)
+        v.copy_(pv)
+        _, e0 = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=0), cams=cams)
+        reach = None
+        for n in range(10, prm.max_iters + 1, 10):
+            u.copy_(pu)
+            v.copy_(pv)
+            _, e = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=n), dual_sigma=dual_sigma, cams=cams)
+            if e <= e_p:
+                reach = n
+                break
+        rows.append(dict(seed=int(s), plain_ms=ms_p, plain_iters=it_p, plain_energy=e_p, plain_err=err_p,
+                         warm_ms=ms_w, warm_iters=it_w, warm_energy=e_w, warm_err=err_w, start_energy=e0,
+                         warm_iters_to_plain_energy=reach))
+        if log:
+            log(rows[-1])
+    return rows
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--scenes", type=int, default=2000)
+    t.add_argument("--first-seed", type=int, default=10_000)
+    t.add_argument("--target-iters", type=int, default=3000)
+    t.add_argument("--steps", type=int, default=4000)
+    t.add_argument("--batch", type=int, default=4)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--norm", type=float, nargs=7, default=None)
+    t.add_argument("--out", default=str(WEIGHTS))
+    a = ap.parse_args(argv)
+    import mvs_b200 as M
+    cfg = FrameConfig()
+    norm = tuple(a.norm) if a.norm else M.UNET_DEFAULT_NORM
+    data = make_dataset(range(a.first_seed, a.first_seed + a.scenes), cfg, a.target_iters, log=print)
+    params, losses = train(data, a.steps, a.batch, a.lr, norm=norm, log=print)
+    meta = dict(scenes=a.scenes, first_seed=a.first_seed, target_iters=a.target_iters, steps=a.steps,
+                batch=a.batch, lr=a.lr, final_loss=float(np.mean(losses[-100:])))
+    save_weights(a.out, params, norm, meta)
+    print("saved", a.out, meta)
+
+
+if __name__ == "__main__":
+    main()
