@@ -164,6 +164,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["mvs", "reference"], default="mvs")
     ap.add_argument("--tgv-steps", type=int, default=3)
+    ap.add_argument("--no-warm-start", dest="warm_start", action="store_false",
+                    help="skip the learned TGV2 warm start")
+    ap.add_argument("--warm-frames", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fusion", dest="fusion", action="store_false")
     ap.add_argument("--fusion-dims", type=int, default=256, help="voxels per side of the fusion volume")
@@ -267,6 +270,31 @@ def main():
         if k > 0:
             tgv_ms.append(a.elapsed_time(b))
     tgv_ms_frame = dist.max_over_ranks(statistics.mean(tgv_ms), dev) if tgv_ms else None
+
+    # --- learned warm start: network prediction from (WTA depth, cost, image), then
+    #     TGV2 from it with the same linearisation (WTA depth), tolerance and cap, against plain
+    #     TGV2 from the WTA depth (the judge), averaged over held-out frames of configs[1] ---
+    warm = None
+    if tgv_ms and args.warm_start:
+        from mvs_b200 import warmstart as WS
+        wparams, wnorm, wmeta = WS.load_weights()
+        rows = WS.evaluate(range(920000 + 100 * rank, 920000 + 100 * rank + args.warm_frames), WS.FrameConfig(),
+                           wparams, wnorm, device=dev)
+        pm = statistics.mean(r["plain_ms"] for r in rows)
+        wm = statistics.mean(r["warm_ms"] for r in rows)
+        pm, wm = dist.max_over_ranks(pm, dev), dist.max_over_ranks(wm, dev)
+        er = [r["warm_energy"] / r["plain_energy"] - 1.0 for r in rows]
+        warm = {"frames": len(rows), "ms_per_frame_plain": pm, "ms_per_frame": wm, "speedup_vs_plain": pm / wm,
+                "iterations_plain": [r["plain_iters"] for r in rows],
+                "iterations_warm": [r["warm_iters"] for r in rows],
+                "warm_iterations_to_plain_energy": [r["warm_iters_to_plain_energy"] for r in rows],
+                "energy_rel_to_plain_mean": statistics.mean(er), "energy_rel_to_plain_max": max(er),
+                "frames_with_fallback_to_plain": sum(e > 1e-4 for e in er),
+                "median_abs_depth_err_m": {"plain": statistics.mean(r["plain_err"] for r in rows),
+                                           "warm": statistics.mean(r["warm_err"] for r in rows)},
+                "dual_start": {"sigma_pq": WS.WARM_DUAL_SIGMA, "sigma_r": WS.WARM_DUAL_SIGMA_R},
+                "network": {"weights": WS.WEIGHTS.name, "trained": wmeta},
+                "includes": "network forward + TGV2 to tolerance; scenes rendered on the device, seeds held out"}
 
     # --- TV-L1 histogram fusion: 256^3 voxels over a 5 m cube, 40 depthmaps of
     #     640x480 with 1% depth noise and 2% outliers, 7 bins, 200 primal-dual iterations ---
@@ -390,7 +418,8 @@ def main():
                                 "unit": "GB/s", "frac": wta_bytes / (wta_ms / 1e3) / 1e9 / hbm,
                                 "ms_per_launch": wta_ms},
         "tgv2": {"ms_per_frame_plain": tgv_ms_frame, "iterations": tgv_iters, "energy": tgv_e,
-                 "tol": 1e-4, "cap": 500, "start": "WTA depth", "ms_per_frame_warm_start": None},
+                 "tol": 1e-4, "cap": 500, "start": "WTA depth",
+                 "ms_per_frame_warm_start": warm["ms_per_frame"] if warm else None, "warm_start": warm},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": (1 + V) * W * H * 4,
                 "d2h_bytes_per_step": W * H * 4, "api": "mvs_ps_* PlaneSweep handle (RunAlgorithm + getDepthmap)"},
         "fusion": fusion,

@@ -170,15 +170,19 @@ int mvs_tgv2_run(int32_t width, int32_t height, int32_t n_views, const float *d_
  * data term is linearised at d_u_lin (H*W; the plain run's start, e.g. the
  * sweep's winner-take-all depth), so the energy is the plain run's; the
  * primal starts at d_u (H*W, in/out) and d_v (2*H*W, vx then vy, in/out; NULL
- * starts v at 0 and discards it).  dual_sigma > 0 starts p, q and r one dual
- * step of that size from zero (0: at zero, as the plain run).  With d_u equal
- * to d_u_lin, v = 0 and dual_sigma = 0 this is mvs_tgv2_run with
- * u_from_input = 1.  Later linearisations (warps > 1) restart as the plain
- * run does. */
+ * starts v at 0 and discards it).  dual_sigma > 0 starts the regulariser's
+ * duals p, q, and dual_sigma_r > 0 the data duals r, one dual step of that
+ * size from zero (0: at zero, as the plain run; a large dual_sigma_r starts r
+ * at the sign of each view's residual).  d_pq (5*H*W: px, py, qx, qy, qz)
+ * and d_r (n_views*H*W), when not NULL, are instead the start of those duals
+ * and receive their final values, so a run can continue another exactly.
+ * With d_u equal to d_u_lin, v = 0 and both steps 0 this is mvs_tgv2_run
+ * with u_from_input = 1.  Later linearisations (warps > 1) restart as the
+ * plain run does. */
 int mvs_tgv2_run_warm(int32_t width, int32_t height, int32_t n_views, const float *d_ref255, const float *d_srcs255,
                       const float *h_K9, const float *h_invK9, const float *h_Rrel, const float *h_trel,
                       const mvs_tgv2_params *params, const float *d_u_lin, float *d_u, float *d_v, double dual_sigma,
-                      int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
+                      double dual_sigma_r, float *d_pq, float *d_r, int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
                       void *stream);
 
 /* ---- TV-L1 depth denoise --------------------------------------------------

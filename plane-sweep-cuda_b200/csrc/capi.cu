@@ -223,7 +223,8 @@ int mvs_tgv2_run(int32_t w, int32_t h, int32_t V, const float *ref255, const flo
 
 int mvs_tgv2_run_warm(int32_t w, int32_t h, int32_t V, const float *ref255, const float *srcs255, const float *K9,
                       const float *invK9, const float *Rrel, const float *trel, const mvs_tgv2_params *prm,
-                      const float *u_lin, float *u, float *v, double dual_sigma, int32_t *iters_out,
+                      const float *u_lin, float *u, float *v, double dual_sigma, double dual_sigma_r,
+                      float *pq, float *r, int32_t *iters_out,
                       double *energy_out, void *ws, size_t ws_bytes, void *stream)
 {
     clear_error();
@@ -231,10 +232,10 @@ int mvs_tgv2_run_warm(int32_t w, int32_t h, int32_t V, const float *ref255, cons
     if (!ref255 || !srcs255 || !K9 || !invK9 || !Rrel || !trel || !prm || !u || !u_lin)
         return set_error(MVS_ERR_ARG, "null pointer");
     if (prm->niters < 0 || prm->warps < 0) return set_error(MVS_ERR_ARG, "negative iteration count");
-    if (!(dual_sigma >= 0)) return set_error(MVS_ERR_ARG, "dual_sigma must be >= 0");
+    if (!(dual_sigma >= 0) || !(dual_sigma_r >= 0)) return set_error(MVS_ERR_ARG, "dual steps must be >= 0");
     const size_t need = tgv2_workspace_bytes(w, h, V);
     if (!ws || ws_bytes < need) return set_error(MVS_ERR_ARG, "workspace of %zu bytes needed", need);
-    TGV2Warm warm{u_lin, v, dual_sigma};
+    TGV2Warm warm{u_lin, v, dual_sigma, dual_sigma_r, pq, r};
     int it = 0;
     int rc = tgv2_run(w, h, V, ref255, srcs255, K9, invK9, Rrel, trel, prm, 1, 0.f, u, &it, energy_out, ws,
                       (cudaStream_t)stream, &warm);

@@ -57,11 +57,15 @@ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 // Warm start of a TGV2 run: the data term is linearised at u_lin (first
 // linearisation) while the primal starts at the caller's u and at v (2 planes,
 // vx then vy; NULL = 0), which also receives the final v.  dual_sigma > 0
-// starts the dual variables one dual step of that size from zero.
+// (dual_sigma_r > 0) starts the regulariser's (the data term's) dual
+// variables one dual step of that size from zero.  pq (5 planes: px, py, qx,
+// qy, qz) and r (one plane per view), when given, are the duals' start
+// instead and receive their final values.
 struct TGV2Warm {
     const float *u_lin;
     float *v;
-    double dual_sigma;
+    double dual_sigma, dual_sigma_r;
+    float *pq, *r;
 };
 
 }  // namespace mvs

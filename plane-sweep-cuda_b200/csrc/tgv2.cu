@@ -94,7 +94,8 @@ __global__ void warm_init_kernel(int n, int V, const float *__restrict__ u_lin, 
                                  float *__restrict__ ubar, float *__restrict__ u1x, float *__restrict__ u1y,
                                  float *__restrict__ u1xbar, float *__restrict__ u1ybar, float *__restrict__ Px,
                                  float *__restrict__ Py, float *__restrict__ Qx, float *__restrict__ Qy,
-                                 float *__restrict__ Qz, float *__restrict__ r)
+                                 float *__restrict__ Qz, float *__restrict__ r, const float *__restrict__ pq_in,
+                                 const float *__restrict__ r_in)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         u0[i] = u_lin[i];
@@ -102,8 +103,16 @@ __global__ void warm_init_kernel(int n, int V, const float *__restrict__ u_lin, 
         const float a = vx ? vx[i] : 0.f, c = vy ? vy[i] : 0.f;
         u1x[i] = u1xbar[i] = a;
         u1y[i] = u1ybar[i] = c;
-        Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
-        for (int k = 0; k < V; ++k) r[(size_t)k * n + i] = 0.f;
+        if (pq_in) {
+            Px[i] = pq_in[i];
+            Py[i] = pq_in[(size_t)n + i];
+            Qx[i] = pq_in[2 * (size_t)n + i];
+            Qy[i] = pq_in[3 * (size_t)n + i];
+            Qz[i] = pq_in[4 * (size_t)n + i];
+        } else {
+            Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
+        }
+        for (int k = 0; k < V; ++k) r[(size_t)k * n + i] = r_in ? r_in[(size_t)k * n + i] : 0.f;
     }
 }
 
@@ -375,26 +384,27 @@ __global__ void sum_partials_kernel(const double *__restrict__ partial, int m, d
     }
 }
 
-// Dual start for a warm-started primal: one dual step of size sd from zero,
-// p = P(a1 sd T(grad u - v)), q = P(a0 sd e(v)), r_i = P(sd lambda (It_i +
-// (u - u0) Iu_i)), with the iteration's projections.  For a large sd this puts
-// each dual variable at the unit direction of its term, its value at the
-// saddle point wherever that term is non-zero.
+// Dual start for a warm-started primal: one dual step from zero, of size sd
+// for the regulariser's duals and sdr for the data duals:
+// p = P(a1 sd T(grad u - v)), q = P(a0 sd e(v)), r_i = P(sdr lambda (It_i +
+// (u - u0) Iu_i)), with the iteration's projections.  A large step puts a dual
+// variable at the unit direction of its term, its value at the saddle point
+// wherever that term is non-zero (for r: the sign of the residual).
 __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
                                  const float *__restrict__ T22, const float *__restrict__ It,
                                  const float *__restrict__ Iu, const float *__restrict__ u0,
                                  const float *__restrict__ u, const float *__restrict__ u1x,
                                  const float *__restrict__ u1y, int w, int h, int V, float lambda, float alpha0,
-                                 float alpha1, float sd, float *__restrict__ Px, float *__restrict__ Py,
+                                 float alpha1, float sd, float sdr, float *__restrict__ Px, float *__restrict__ Py,
                                  float *__restrict__ Qx, float *__restrict__ Qy, float *__restrict__ Qz,
-                                 float *__restrict__ r)
+                                 float *__restrict__ r, int do_pq, int do_r)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     const size_t n = (size_t)w * h;
     const int i = y * w + x, xn = min(x + 1, w - 1), yn = min(y + 1, h - 1);
     const int ix = y * w + xn, iy = yn * w + x;
-    {
+    if (do_pq) {
         const double xg = (double)u[ix] - u[i] - u1x[i];
         const double yg = (double)u[iy] - u[i] - u1y[i];
         const double s = (double)alpha1 * sd;
@@ -403,7 +413,7 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
         Px[i] = (float)(dx / d);
         Py[i] = (float)(dy / d);
     }
-    {
+    if (do_pq) {
         const double s = (double)alpha0 * sd;
         const double dx = s * ((double)u1x[ix] - u1x[i]);
         const double dy = s * ((double)u1y[iy] - u1y[i]);
@@ -413,10 +423,11 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
         Qy[i] = (float)(dy / d);
         Qz[i] = (float)(dz / d);
     }
+    if (!do_r) return;
     const float du = u[i] - u0[i];
     for (int v = 0; v < V; ++v) {
         const size_t k = (size_t)v * n + i;
-        float q = sd * lambda * (It[k] + du * Iu[k]);
+        float q = sdr * lambda * (It[k] + du * Iu[k]);
         r[k] = q / fmaxf(1.f, fabsf(q));
     }
 }
@@ -503,6 +514,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     int total = 0;
     double last_e = 0.0;
     int energy_at = -1;   // iteration count at which last_e was evaluated
+    int cur = 0;          // ping-pong buffer holding the current p, q
     bool done = false;
     IterBufs ib;
     ib.T11 = L.T11;
@@ -528,18 +540,22 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         if (warm && l == 0)
             warm_init_kernel<<<eg, 256, 0, st>>>(n, V, warm->u_lin, u, warm->v, warm->v ? warm->v + n : nullptr, L.u0,
                                                 L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0], L.Px[0], L.Py[0],
-                                                L.Qx[0], L.Qy[0], L.Qz[0], L.r);
+                                                L.Qx[0], L.Qy[0], L.Qz[0], L.r, warm->pq, warm->r);
         else
             warp_init_kernel<<<eg, 256, 0, st>>>(n, V, u, L.u0, L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0],
                                                 L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0], L.r);
         linearize_kernel<<<dim3(g2.x, g2.y, V), b2, 0, st>>>(cams, srcs255, L.ref01, L.u0, w, h, L.It, L.Iu);
-        if (warm && l == 0 && warm->dual_sigma > 0)
-            dual_init_kernel<<<g2, b2, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
-                                               prm->lambda, prm->alpha0, prm->alpha1, (float)warm->dual_sigma,
-                                               L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0], L.r);
+        if (warm && l == 0) {
+            const int do_pq = !warm->pq && warm->dual_sigma > 0, do_r = !warm->r && warm->dual_sigma_r > 0;
+            if (do_pq || do_r)
+                dual_init_kernel<<<g2, b2, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
+                                                   prm->lambda, prm->alpha0, prm->alpha1, (float)warm->dual_sigma,
+                                                   (float)warm->dual_sigma_r, L.Px[0], L.Py[0], L.Qx[0], L.Qy[0],
+                                                   L.Qz[0], L.r, do_pq, do_r);
+        }
         rc = check_launch("tgv2 linearisation");
         if (rc) break;
-        int cur = 0;
+        cur = 0;
         bool have_prev = false;
         double prev = 0.0;
         for (int k = 0; k < prm->niters; ++k) {
@@ -597,6 +613,16 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         cudaMemcpyAsync(warm->v, L.u1x, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(warm->v + n, L.u1y, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
         rc = check_launch("tgv2 v readout");
+    }
+    if (!rc && warm && warm->pq) {
+        float *const src[5] = {L.Px[cur], L.Py[cur], L.Qx[cur], L.Qy[cur], L.Qz[cur]};
+        for (int k = 0; k < 5; ++k)
+            cudaMemcpyAsync(warm->pq + (size_t)k * n, src[k], n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        rc = check_launch("tgv2 dual readout");
+    }
+    if (!rc && warm && warm->r) {
+        cudaMemcpyAsync(warm->r, L.r, (size_t)V * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        rc = check_launch("tgv2 dual readout");
     }
     if (!rc && energy_out && energy_at != total) {
         // energy of the final iterate for callers that ask for it

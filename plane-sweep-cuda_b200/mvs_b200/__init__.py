@@ -97,7 +97,7 @@ _sig("mvs_tgv2_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32, C.c_int32)
 _sig("mvs_tgv2_run", C.c_int, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _F, _F, _F, _F, C.POINTER(TGV2Params),
      C.c_int32, C.c_float, _VP, _I32, _D, _VP, C.c_size_t, _VP)
 _sig("mvs_tgv2_run_warm", C.c_int, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _F, _F, _F, _F, C.POINTER(TGV2Params),
-     _VP, _VP, _VP, C.c_double, _I32, _D, _VP, C.c_size_t, _VP)
+     _VP, _VP, _VP, C.c_double, C.c_double, _VP, _VP, _I32, _D, _VP, C.c_size_t, _VP)
 _sig("mvs_render_scene", C.c_int, C.POINTER(BoxSceneDesc), _D, _D, _D, C.c_int32, C.c_int32, _VP, _VP, _VP)
 _sig("mvs_unet_create", C.c_int, C.POINTER(_VP), C.c_int32, C.c_int32, C.c_int32, _F)
 _sig("mvs_unet_destroy", C.c_int, _VP)
@@ -273,10 +273,11 @@ def tgv2_run(ref255, srcs255, K9, invK9, Rrel, trel, params, u, u_from_input=Fal
 
 
 def tgv2_run_warm(ref255, srcs255, K9, invK9, Rrel, trel, params, u_lin, u, v=None, dual_sigma=0.0,
-                  workspace=None, stream=None):
+                  dual_sigma_r=0.0, pq=None, r=None, workspace=None, stream=None):
     """TGV2 linearised at ``u_lin`` with the primal started at ``u`` (in/out)
-    and ``v`` ((2, H, W), in/out, or None for 0).  Returns (iterations,
-    final energy)."""
+    and ``v`` ((2, H, W), in/out, or None for 0); optional dual state ``pq``
+    ((5, H, W)) and ``r`` ((V, H, W)), in/out.  Returns (iterations, final
+    energy)."""
     h, w = ref255.shape[-2:]
     V = srcs255.shape[0]
     it = C.c_int32(0)
@@ -284,7 +285,8 @@ def tgv2_run_warm(ref255, srcs255, K9, invK9, Rrel, trel, params, u_lin, u, v=No
     ws_bytes = 0 if workspace is None else workspace.numel() * workspace.element_size()
     K9, invK9, Rrel, trel = (_f32(x) for x in (K9, invK9, Rrel, trel))
     check(_L.mvs_tgv2_run_warm(w, h, V, _ptr(ref255), _ptr(srcs255), _fp(K9), _fp(invK9), _fp(Rrel), _fp(trel),
-                               C.byref(params), _ptr(u_lin), _ptr(u), _ptr(v), float(dual_sigma), C.byref(it),
+                               C.byref(params), _ptr(u_lin), _ptr(u), _ptr(v), float(dual_sigma),
+                               float(dual_sigma_r), _ptr(pq), _ptr(r), C.byref(it),
                                C.byref(e), _ptr(workspace), ws_bytes, _stream(stream)))
     return it.value, e.value
 

@@ -29,6 +29,11 @@ from . import hostmath as hm
 from . import scenes
 
 WEIGHTS = pathlib.Path(__file__).resolve().parent / "warmstart_weights.npz"
+# dual start of the warm-started run: a small step for p, q and a moderate one
+# for the data duals r (a large one puts every view's r at the sign of its
+# residual, wrong for the view whose residual the L1 optimum zeroes)
+WARM_DUAL_SIGMA = 0.1
+WARM_DUAL_SIGMA_R = 5.0
 
 
 @dataclasses.dataclass
@@ -94,11 +99,13 @@ class Pipeline:
                            self.cfg.zfar, self.depth, self.labels, self.best)
         return self.depth, self.best
 
-    def tgv(self, frame, u_lin, u, v, prm, dual_sigma=0.0, cams=None):
-        """TGV2 linearised at u_lin from (u, v) (both in/out).  (iterations, energy)."""
+    def tgv(self, frame, u_lin, u, v, prm, dual_sigma=0.0, dual_sigma_r=0.0, cams=None, pq=None, r=None):
+        """TGV2 linearised at u_lin from (u, v) (both in/out) and optionally the
+        duals (pq, r; in/out).  (iterations, energy)."""
         c = cams or self.cams(frame)
         return self.M.tgv2_run_warm(frame.ref, frame.srcs, c["Kf"], c["iK"], c["Rs"], c["ts"], prm, u_lin, u, v,
-                                    dual_sigma=dual_sigma, workspace=self.tws)
+                                    dual_sigma=dual_sigma, dual_sigma_r=dual_sigma_r, pq=pq, r=r,
+                                    workspace=self.tws)
 
 
 def make_dataset(seeds, cfg: FrameConfig, target_iters: int, device="cuda", log=None):
@@ -194,7 +201,8 @@ class WarmStart:
         return self.u[0], self.v[0]
 
 
-def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=0.0, device="cuda", log=None):
+def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=WARM_DUAL_SIGMA,
+             dual_sigma_r=WARM_DUAL_SIGMA_R, device="cuda", log=None, reach=True):
     """Plain TGV2 (from the winner-take-all depth) against the warm-started run
     (network prediction, same linearisation and stopping rule) on `seeds`.
 
@@ -237,7 +245,7 @@ def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=0.0, de
         pu, pv = ws.predict(wta[None], cost[None], fr.ref[None])
         u.copy_(pu)
         v.copy_(pv)
-        it_w, e_w = pipe.tgv(fr, wta, u, v, prm, dual_sigma=dual_sigma, cams=cams)
+        it_w, e_w = pipe.tgv(fr, wta, u, v, prm, dual_sigma=dual_sigma, dual_sigma_r=dual_sigma_r, cams=cams)
         b.record()
         torch.cuda.synchronize()
         ms_w = a.elapsed_time(b)
@@ -247,17 +255,18 @@ def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=0.0, de
         u.copy_(pu)
         v.copy_(pv)
         _, e0 = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=0), cams=cams)
-        reach = None
-        for n in range(10, prm.max_iters + 1, 10):
+        n_reach = None
+        for n in (range(10, prm.max_iters + 1, 10) if reach else ()):
             u.copy_(pu)
             v.copy_(pv)
-            _, e = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=n), dual_sigma=dual_sigma, cams=cams)
+            _, e = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=n), dual_sigma=dual_sigma,
+                            dual_sigma_r=dual_sigma_r, cams=cams)
             if e <= e_p:
-                reach = n
+                n_reach = n
                 break
         rows.append(dict(seed=int(s), plain_ms=ms_p, plain_iters=it_p, plain_energy=e_p, plain_err=err_p,
                          warm_ms=ms_w, warm_iters=it_w, warm_energy=e_w, warm_err=err_w, start_energy=e0,
-                         warm_iters_to_plain_energy=reach))
+                         warm_iters_to_plain_energy=n_reach))
         if log:
             log(rows[-1])
     return rows
