@@ -321,6 +321,55 @@ typedef struct mvs_box_scene {
 int mvs_render_scene(const mvs_box_scene *scene, const double *h_invK9, const double *h_R9, const double *h_center3,
                      int32_t width, int32_t height, float *d_gray255, float *d_depth, void *stream);
 
+/* ---- batched frames (extension: the reference sweeps one frame per call) --
+ * Many reference frames of any size, view count (<= 16), plane count and
+ * window go through one CUDA-graph launch: FP64 homographies of every
+ * (frame, view, plane), then one persistent sweep kernel over a work list of
+ * (frame, tile, plane chunk) items, in the aggregated mode (cost = 1 - mean
+ * NCC over views, winner-take-all; outputs as mvs_sweep's aggregated mode).
+ * Per-frame completion times are recorded on the device.
+ *
+ * The work list's plane chunk, persistent CTAs per SM and item order come from
+ * `tuning`, or, when it is NULL, from an autotuner that times every candidate
+ * on the batch itself (once per batch shape in a process; the choice is
+ * cached).  Device pointers and K stay the caller's and must outlive the
+ * batch; h_K9 (1-based K), h_Rrel and h_trel (n_views x 9 / x 3, as
+ * mvs_sweep_homographies takes them) are read at creation. */
+#define MVS_BATCH_ORDER_FRAME 0          /* frame by frame, in the given order */
+#define MVS_BATCH_ORDER_LARGEST_FIRST 1  /* frame by frame, most work first */
+#define MVS_BATCH_ORDER_INTERLEAVED 2    /* round robin over frames */
+
+typedef struct mvs_batch_frame {
+    int32_t width, height, n_views, n_planes, window;
+    float std_threshold, zfar;
+    const float *d_ref, *d_srcs, *d_depths;   /* H*W, n_views*H*W (0..255), n_planes */
+    const double *h_K9, *h_Rrel, *h_trel;
+    float *d_depth;                           /* outputs, H*W; labels and best may be NULL */
+    int32_t *d_labels;
+    float *d_best;
+} mvs_batch_frame;
+
+typedef struct mvs_batch_tuning {
+    int32_t planes_per_chunk;   /* 0: whole plane range per item */
+    int32_t ctas_per_sm;        /* persistent CTAs per SM (1 or 2) */
+    int32_t order;              /* MVS_BATCH_ORDER_* */
+} mvs_batch_tuning;
+
+typedef struct mvs_batch mvs_batch;
+
+int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, int32_t moments,
+                     const mvs_batch_tuning *tuning);
+int mvs_batch_destroy(mvs_batch *batch);
+int mvs_batch_get_tuning(const mvs_batch *batch, mvs_batch_tuning *tuning);
+/* new relative poses for every frame (views of frame 0 first) */
+int mvs_batch_set_poses(mvs_batch *batch, const double *h_Rrel, const double *h_trel, void *stream);
+/* one graph launch: homographies + sweep + winner-take-all of every frame */
+int mvs_batch_run(mvs_batch *batch, void *stream);
+/* per-frame latency of the last run (ms from the launch's start to the
+ * frame's last tile), after synchronising `stream` */
+int mvs_batch_frame_latency_ms(mvs_batch *batch, float *h_ms, void *stream);
+int64_t mvs_batch_work_items(const mvs_batch *batch);
+
 /* ---- TGV2 warm-start network (no counterpart in the reference) -----------
  * A 4-level U-Net (16/32/64/128 channels, 3x3 convolutions with ReLU, 2x2
  * average pooling, nearest upsampling with skip concatenation, a 1x1 head)
@@ -363,13 +412,14 @@ int mvs_unet_check(mvs_unet *net, void *stream);
  * for checks against a CPU restatement.  d_w: FP32 W[cout][cin][3][3];
  * d_wpack: scratch of 2*9*cin*cout bf16; d_err: device int set on a timeout.
  * backward: d_dw (9*cin*cout) and d_db (cout, may be NULL) are accumulated
- * into; d_dx (may be NULL) = input gradient, times (x > 0) when mask_x. */
+ * into; d_dx (may be NULL) = input gradient, times (x > 0) when mask_x;
+ * tensor_cores = 0 computes the weight gradient on the CUDA cores instead. */
 int mvs_conv3x3_forward(const uint16_t *d_in, int32_t cin, const float *d_w, const float *d_bias, int32_t cout,
                         int32_t batch, int32_t height, int32_t width, int32_t relu, uint16_t *d_out,
                         uint16_t *d_wpack, int32_t *d_err, void *stream);
 int mvs_conv3x3_backward(const uint16_t *d_x, int32_t cin, const float *d_w, const uint16_t *d_dz, int32_t cout,
                          int32_t batch, int32_t height, int32_t width, int32_t mask_x, uint16_t *d_dx, float *d_dw,
-                         float *d_db, uint16_t *d_wpack, int32_t *d_err, void *stream);
+                         float *d_db, uint16_t *d_wpack, int32_t *d_err, int32_t tensor_cores, void *stream);
 
 /* Device time (ms) of the last run_algorithm / tgv / cuda_denoise call,
  * measured with CUDA events around the kernels only. */

@@ -54,6 +54,30 @@ __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// One frame of a batched sweep (device copy; see sweep_batch_kernel).
+struct BatchFrameDev {
+    const float *ref, *srcs, *H, *depths;
+    float *depth;
+    int32_t *labels;
+    float *best;
+    unsigned long long *wta;      // [w*h] winner words, ~0 between launches
+    unsigned int *tile_left;      // [n_tiles] chunks still running
+    unsigned int *frame_left;     // tiles still running
+    unsigned long long *done_ns;  // completion time of the last launch
+    int w, h, V, P, win, planes_per_chunk, n_chunks, tiles_x, n_tiles, tile_w;
+    float stdthresh, zfar;
+};
+
+constexpr int kBatchMaxViews = 16;
+struct BatchCamDev {
+    double K[9], invK[9];
+    double Rrel[kBatchMaxViews][9];
+    double trel[kBatchMaxViews][3];
+    const float *depths;
+    float *H;
+    int V, P;
+};
+
 // Warm start of a TGV2 run: the data term is linearised at u_lin (first
 // linearisation) while the primal starts at the caller's u and at v (2 planes,
 // vx then vy; NULL = 0), which also receives the final v.  dual_sigma > 0

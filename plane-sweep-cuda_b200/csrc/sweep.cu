@@ -472,16 +472,14 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
     }
 }
 
-// ---- aggregated kernel: cost = 1 - mean NCC over views, BF16 WTA -------------------
-// grid: (tiles_x, tiles_y, n_chunks)
+// ---- aggregated mode: cost = 1 - mean NCC over views, BF16 WTA -------------------
+// One CTA's work: tile (tx, ty) of the frame, planes of `chunk`.
 
 template <int WIN, int MOM>
-__global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs a)
+__device__ __forceinline__ void aggregated_tile(Smem &S, const SweepArgs &a, int tx, int ty, int chunk)
 {
     using G = Geo<WIN>;
-    __shared__ Smem S;
-    const int chunk = blockIdx.z;
-    const int x0 = blockIdx.x * G::TW, y0 = blockIdx.y * TH;
+    const int x0 = tx * G::TW, y0 = ty * TH;
     const int w = a.w, h = a.h;
     const size_t n = (size_t)w * h;
 
@@ -563,6 +561,14 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs 
         if (a.n_chunks == 1) *o = key;
         else if (lab[j] >= 0) atomicMin(o, key);
     }
+}
+
+// grid: (tiles_x, tiles_y, n_chunks)
+template <int WIN, int MOM>
+__global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs a)
+{
+    __shared__ Smem S;
+    aggregated_tile<WIN, MOM>(S, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---- epilogues ----------------------------------------------------------------------
@@ -697,6 +703,138 @@ __global__ void homography_kernel(HomCams c, const float *__restrict__ depths, i
     for (int i = 0; i < 9; ++i) H[(size_t)idx * 9 + i] = (float)(O[i] / s);
 }
 
+// ---- batched frames: one persistent launch over a mixed work list ---------------------
+//
+// Work items (frame, tile, plane chunk) of frames of any size, view and plane
+// count and window are handed out by an atomic counter to a grid of
+// persistent CTAs, which run the aggregated sweep on each with the frame's
+// window (a runtime switch over the compiled windows).  The CTA that
+// completes the last chunk of a tile (a per-tile countdown, no waiting)
+// finishes that tile -- winner-take-all word -> depth, label, cost -- and
+// re-arms its scratch for the next launch; the CTA that finishes the last tile
+// of a frame stamps the frame's completion time (%globaltimer).
+
+__device__ __forceinline__ unsigned long long global_timer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void batch_start_kernel(unsigned int *next, unsigned long long *t_start)
+{
+    *next = 0u;
+    *t_start = global_timer_ns();
+}
+
+template <int MOM>
+__global__ void __launch_bounds__(THREADS, 2) sweep_batch_kernel(const BatchFrameDev *__restrict__ frames,
+                                                                  const uint4 *__restrict__ items, int n_items,
+                                                                  unsigned int *next)
+{
+    __shared__ Smem S;
+    __shared__ int s_item, s_last;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(next, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const uint4 item = items[it];   // frame, tile, chunk
+        const BatchFrameDev &f = frames[item.x];
+        SweepArgs a;
+        a.ref = f.ref;
+        a.srcs = f.srcs;
+        a.H = f.H;
+        a.depths = f.depths;
+        a.w = f.w;
+        a.h = f.h;
+        a.V = f.V;
+        a.P = f.P;
+        a.planes_per_chunk = f.planes_per_chunk;
+        a.n_chunks = f.n_chunks;
+        a.stdthresh = f.stdthresh;
+        a.packed = nullptr;
+        a.wta = f.wta;
+        a.cost = nullptr;
+        const int tx = (int)item.y % f.tiles_x, ty = (int)item.y / f.tiles_x;
+        switch (f.win) {
+        case 3: aggregated_tile<3, MOM>(S, a, tx, ty, item.z); break;
+        case 5: aggregated_tile<5, MOM>(S, a, tx, ty, item.z); break;
+        case 7: aggregated_tile<7, MOM>(S, a, tx, ty, item.z); break;
+        case 9: aggregated_tile<9, MOM>(S, a, tx, ty, item.z); break;
+        case 11: aggregated_tile<11, MOM>(S, a, tx, ty, item.z); break;
+        case 13: aggregated_tile<13, MOM>(S, a, tx, ty, item.z); break;
+        default: aggregated_tile<15, MOM>(S, a, tx, ty, item.z); break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();   // this chunk's winner words before the countdown
+            s_last = atomicSub(f.tile_left + item.y, 1u) == 1u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const int tw = f.tile_w, x0 = tx * tw, y0 = ty * TH;
+            for (int k = threadIdx.x; k < tw * TH; k += THREADS) {
+                const int x = x0 + k % tw, y = y0 + k / tw;
+                if (x >= f.w || y >= f.h) continue;
+                const size_t i = (size_t)y * f.w + x;
+                const unsigned long long key = __ldcg(f.wta + i);
+                const bool ok = key != ~0ull;
+                const int lab = ok ? (int)(unsigned)(key & 0xffffffffu) : -1;
+                f.depth[i] = ok ? ldg(f.depths + lab) : f.zfar;
+                if (f.labels) f.labels[i] = lab;
+                if (f.best) f.best[i] = ok ? __uint_as_float((unsigned)(key >> 32)) : 3.f;
+                __stcg(f.wta + i, ~0ull);   // re-armed for the next launch
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                f.tile_left[item.y] = (unsigned)f.n_chunks;
+                __threadfence();
+                if (atomicSub(f.frame_left, 1u) == 1u) {
+                    *f.done_ns = global_timer_ns();
+                    *f.frame_left = (unsigned)f.n_tiles;
+                }
+            }
+        }
+        __syncthreads();   // s_item / s_last are rewritten by the next item
+    }
+}
+
+// FP64 homographies of every (frame, view, plane) of a batch
+__global__ void homography_batch_kernel(const BatchCamDev *__restrict__ cams, const int *__restrict__ offsets,
+                                        int n_frames)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= offsets[n_frames]) return;
+    int f = 0;
+    while (offsets[f + 1] <= idx) ++f;   // frames are few
+    const BatchCamDev &c = cams[f];
+    const int k = idx - offsets[f];
+    const int v = k / c.P, p = k % c.P;
+    const double d = (double)c.depths[p];
+    const double *R = c.Rrel[v], *t = c.trel[v];
+    double M[9], T[9], O[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) M[i] = R[i];
+    M[2] += t[0] / d;
+    M[5] += t[1] / d;
+    M[8] += t[2] / d;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = fma(c.K[3 * i], M[j], fma(c.K[3 * i + 1], M[3 + j], c.K[3 * i + 2] * M[6 + j]));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            O[3 * i + j] = fma(T[3 * i], c.invK[j], fma(T[3 * i + 1], c.invK[3 + j], T[3 * i + 2] * c.invK[6 + j]));
+    const double sc = O[8];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) c.H[(size_t)k * 9 + i] = (float)(O[i] / sc);
+}
+
 template <int MOM>
 int launch_window(int win, const SweepArgs &a, int mode, void *stream)
 {
@@ -783,6 +921,23 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
         wta_finish_kernel<<<eg, eb, 0, st>>>(scratch, depths, n, d->zfar, depth, labels, best);
     }
     return check_launch("sweep epilogue");
+}
+
+int sweep_tile_width(int win) { return ((RWMAX - 2 * (win / 2)) / 8) * 8; }
+int sweep_tile_height() { return TH; }
+
+int sweep_batch_launch(const BatchFrameDev *frames, const uint4 *items, int n_items, unsigned int *next,
+                       unsigned long long *t_start, const BatchCamDev *cams, const int *hom_offsets, int n_frames,
+                       int n_hom, int moments, int ctas, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    batch_start_kernel<<<1, 1, 0, st>>>(next, t_start);
+    if (n_hom > 0) homography_batch_kernel<<<ceil_div(n_hom, 128), 128, 0, st>>>(cams, hom_offsets, n_frames);
+    if (moments == MVS_MOMENTS_REFERENCE)
+        sweep_batch_kernel<MVS_MOMENTS_REFERENCE><<<ctas, THREADS, 0, st>>>(frames, items, n_items, next);
+    else
+        sweep_batch_kernel<MVS_MOMENTS_COMPENSATED><<<ctas, THREADS, 0, st>>>(frames, items, n_items, next);
+    return check_launch("sweep batch");
 }
 
 int sweep_wta_volume(const uint16_t *cost, const float *depths, int n, int P, float zfar, float *depth,

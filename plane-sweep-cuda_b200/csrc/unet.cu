@@ -171,6 +171,12 @@ struct ConvArgs {
 
 constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s
 
+#define MVS_RC_(x)                \
+    do {                          \
+        int rc__ = (x);           \
+        if (rc__) return rc__;    \
+    } while (0)
+
 template <int COUT>
 struct ConvSmem {
     static constexpr int W_BYTES = 9 * 2 * COUT * 16;
@@ -348,7 +354,198 @@ int launch_conv(const bf16 *in, int cin, const bf16 *wpack, const float *bias, c
 }
 
 // ---------------------------------------------------------------------------
+// weight gradient on tensor cores: for every tap t,
+//   D_t[co][ci] += sum_p dz[p][co] * x[p + off_t][ci]
+// with K = pixels.  A = dz^T (M = co, padded to 128 rows of zeros) and
+// B = x_t^T (N = a chunk of NC input channels) are both MN-major: in shared
+// memory dz sits as [co/8][pixel][8] and x as the same halo tile as the
+// forward pass, [ci/8][halo pixel][8], so one K step of 16 pixels (two tile
+// rows) of tap t is the halo addressed from tap t's offset.  Each CTA sums a
+// run of pixel tiles into 9 accumulators (9 x NC TMEM columns) and adds them
+// to the FP32 gradient with one atomic per weight.
+// ---------------------------------------------------------------------------
+
+struct WgArgs {
+    const bf16 *x;    // [B][H][W][cin]
+    const bf16 *dz;   // [B][H][W][cout]
+    float *dW;        // [cout][cin][9]
+    int *err;
+    int B, H, W, cin, cout, tiles_x, tiles_y, tiles_per_cta, n_tiles;
+};
+
+constexpr int WG_TC_THREADS = 128;
+
+template <int NC>
+struct WgSmem {
+    static constexpr int A_BYTES = 16 * 128 * 16;            // 16 co8 groups x 128 pixels x 16 B
+    static constexpr int B_BYTES = (NC / 8) * HALO_PIX * 16;
+    static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr int USED = 2 * STAGE + 64;
+    // at least 116 KB so that one CTA holds an SM (its 512 TMEM columns)
+    static constexpr int BYTES = USED > 116 * 1024 ? USED : 116 * 1024;
+};
+
+// MN-major descriptors have the instruction descriptor's transpose bits set
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) { return idesc_bf16(M, N) | (1u << 15) | (1u << 16); }
+
+template <int NC>
+__global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
+{
+    using S = WgSmem<NC>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = (uint64_t *)(smem + 2 * S::STAGE);
+    uint32_t *tmem_slot = (uint32_t *)(smem + 2 * S::STAGE + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ci0 = blockIdx.y * NC, co0 = blockIdx.z * 128;
+    const int t_begin = blockIdx.x * a.tiles_per_cta;
+    const int t_end = min(t_begin + a.tiles_per_cta, a.n_tiles);
+    const int H = a.H, W = a.W, cin = a.cin, cout = a.cout;
+    const size_t img = (size_t)H * W;
+    constexpr int TMEM_COLS = 9 * NC <= 256 ? 256 : 512;
+
+    if (warp == 0) tmem_alloc(tmem_slot, TMEM_COLS);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // rows co >= cout of A stay zero in both stages
+    for (int k = tid; k < 2 * S::STAGE / 16; k += WG_TC_THREADS) ((uint4 *)smem)[k] = make_uint4(0, 0, 0, 0);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t sbase = smem_u32(smem);
+
+    auto load = [&](int tile, int s) {
+        const int b = tile / (a.tiles_x * a.tiles_y), r = tile - b * a.tiles_x * a.tiles_y;
+        const int y0 = (r / a.tiles_x) * TH, x0 = (r % a.tiles_x) * TW;
+        const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
+        const int cg = min(cout - co0, 128) >> 3;
+        for (int k = tid; k < cg * 128; k += WG_TC_THREADS) {
+            const int g = k >> 7, m = k & 127;
+            const int gy = y0 + (m >> 3), gx = x0 + (m & 7);
+            const bool ok = gy < H && gx < W;
+            const bf16 *src = a.dz + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cout + co0 + 8 * g;
+            cp_async16(ab + (g * 128 + m) * 16, src, ok);
+        }
+        for (int k = tid; k < (NC / 8) * HALO_PIX; k += WG_TC_THREADS) {
+            const int g = k / HALO_PIX, pix = k - g * HALO_PIX;
+            const int hy = pix / HW_, hx = pix - hy * HW_;
+            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
+            const bool ok = gy >= 0 && gy < H && gx >= 0 && gx < W;
+            const bf16 *src = a.x + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + ci0 + 8 * g;
+            cp_async16(bb + (g * HALO_PIX + pix) * 16, src, ok);
+        }
+        cp_async_wait_all();
+        fence_async_smem();
+    };
+
+    constexpr uint32_t idesc = idesc_bf16_mn(128, NC);
+    const int n = t_end - t_begin;
+    bool failed = false;
+    if (n > 0) {
+        load(t_begin, 0);
+        __syncthreads();
+    }
+    for (int c = 0; c < n; ++c) {
+        const int s = c & 1;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
+#pragma unroll 1
+            for (int t = 0; t < 9; ++t) {
+                const int ky = t / 3, kx = t - 3 * ky;
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks) {
+                    const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
+                    const uint64_t bd = smem_desc(bb + ((2 * ks + ky) * HW_ + kx) * 16, HW_ * 16, HALO_PIX * 16);
+                    mma_bf16(tmem + t * NC, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+                }
+            }
+            mma_commit(&bars[s]);
+        }
+        if (c + 1 < n) {
+            if (c >= 1) {
+                const bool ok = mbar_wait_bounded(&bars[s ^ 1], ((c - 1) >> 1) & 1, kWaitNs);
+                failed = __syncthreads_or(!ok) != 0;
+                if (failed) break;
+            }
+            load(t_begin + c + 1, s ^ 1);
+            __syncthreads();
+        }
+    }
+    if (!failed && n > 0) {
+        const bool ok = mbar_wait_bounded(&bars[(n - 1) & 1], ((n - 1) >> 1) & 1, kWaitNs);
+        failed = __syncthreads_or(!ok) != 0;
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(a.err, 1);
+        mbar_wait_bounded(&bars[(n - 1) & 1], ((n - 1) >> 1) & 1, kWaitNs);
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) {
+            tc_fence_after();
+            tmem_dealloc(tmem, TMEM_COLS);
+        }
+        return;
+    }
+    tc_fence_after();
+    if (n > 0) {
+        const int co = co0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int t = 0; t < 9; ++t) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < NC; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + t * NC + c0, v);
+                if (co < cout) {
+                    float *dst = a.dW + ((size_t)co * cin + ci0 + c0) * 9 + t;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) atomicAdd(dst + 9 * j, v[j]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+template <int NC>
+int launch_wgrad_tc_t(WgArgs a, int n_chunks, cudaStream_t st)
+{
+    using S = WgSmem<NC>;
+    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
+    const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
+    wgrad_tc_kernel<NC><<<dim3(ctas, n_chunks, ceil_div(a.cout, 128)), WG_TC_THREADS, S::BYTES, st>>>(a);
+    return MVS_OK;
+}
+
+int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, int *err,
+                    cudaStream_t st)
+{
+    if (cout % 8 || cin % 16) return set_error(MVS_ERR_ARG, "wgrad: cin %d, cout %d", cin, cout);
+    const int nc = cin % 48 == 0 ? 48 : cin % 32 == 0 ? 32 : 16;
+    WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0};
+    a.n_tiles = B * a.tiles_x * a.tiles_y;
+    const int chunks = cin / nc;
+    // about two waves of CTAs over the SMs
+    a.tiles_per_cta = std::max(1, a.n_tiles * chunks / (2 * kSMs));
+    switch (nc) {
+    case 16: return launch_wgrad_tc_t<16>(a, chunks, st);
+    case 32: return launch_wgrad_tc_t<32>(a, chunks, st);
+    default: return launch_wgrad_tc_t<48>(a, chunks, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // weight gradient (CUDA cores, FP32): dW[co][ci][t] += sum_p x[p + off_t][ci] dz[p][co]
+// (the reference formulation the tensor-core kernel is tested against)
 // ---------------------------------------------------------------------------
 
 constexpr int WG_THREADS = 256;
@@ -430,8 +627,24 @@ __global__ void bgrad_kernel(const bf16 *__restrict__ dz, long long npix, int co
     }
 }
 
-int launch_wgrad(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, float *db,
-                 cudaStream_t st)
+int launch_wgrad_cuda_cores(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW,
+                            cudaStream_t st);
+
+int launch_wgrad(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, float *db, int *err,
+                 cudaStream_t st, bool tensor_cores = true)
+{
+    const long long npix = (long long)B * H * W;
+    if (tensor_cores) {
+        MVS_RC_(launch_wgrad_tc(x, cin, dz, cout, B, H, W, dW, err, st));
+    } else {
+        MVS_RC_(launch_wgrad_cuda_cores(x, cin, dz, cout, B, H, W, dW, st));
+    }
+    if (db) bgrad_kernel<<<(int)((npix + 2047) / 2048), 256, 0, st>>>(dz, npix, cout, 2048, db);
+    return MVS_OK;
+}
+
+int launch_wgrad_cuda_cores(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW,
+                            cudaStream_t st)
 {
     const long long npix = (long long)B * H * W;
     const int px = 4096;
@@ -445,7 +658,6 @@ int launch_wgrad(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H,
     MVS_WG(16, 16) MVS_WG(16, 32) MVS_WG(16, 64) MVS_WG(32, 16) MVS_WG(32, 32) MVS_WG(32, 64) MVS_WG(64, 16)
     MVS_WG(64, 32) MVS_WG(64, 64) return set_error(MVS_ERR_ARG, "wgrad tile %dx%d", tci, tco);
 #undef MVS_WG
-    if (db) bgrad_kernel<<<(int)((npix + 2047) / 2048), 256, 0, st>>>(dz, npix, cout, 2048, db);
     return MVS_OK;
 }
 
@@ -917,7 +1129,7 @@ int conv_bwd(mvs_unet *n, int l, const bf16 *x, const bf16 *dz, bf16 *dx, bool m
 {
     const ConvLayer &c = n->L[l];
     const int H = n->H >> lvl, W = n->W >> lvl;
-    MVS_RC(launch_wgrad(x, c.cin, dz, c.cout, n->B, H, W, n->grads + c.w_off, n->grads + c.b_off, st));
+    MVS_RC(launch_wgrad(x, c.cin, dz, c.cout, n->B, H, W, n->grads + c.w_off, n->grads + c.b_off, n->err, st));
     if (dx)
         MVS_RC(launch_conv(dz, c.cout, c.wb, nullptr, mask_x ? x : nullptr, dx, c.cin, n->B, H, W, 0, n->err, st));
     return MVS_OK;
@@ -1134,14 +1346,14 @@ int mvs_conv3x3_forward(const uint16_t *d_in, int32_t cin, const float *d_w, con
 
 int mvs_conv3x3_backward(const uint16_t *d_x, int32_t cin, const float *d_w, const uint16_t *d_dz, int32_t cout,
                          int32_t batch, int32_t height, int32_t width, int32_t mask_x, uint16_t *d_dx, float *d_dw,
-                         float *d_db, uint16_t *d_wpack, int32_t *d_err, void *stream)
+                         float *d_db, uint16_t *d_wpack, int32_t *d_err, int32_t tensor_cores, void *stream)
 {
     if (!d_x || !d_w || !d_dz || !d_dw || !d_wpack || !d_err) return set_error(MVS_ERR_ARG, "null argument");
     if (cout % 16 || cin % 16) return set_error(MVS_ERR_ARG, "channels must be multiples of 16");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t s = (size_t)9 * cin * cout;
     pack_kernel<<<ceil_div((int)s, 256), 256, 0, st>>>(d_w, cin, cout, d_wpack, d_wpack + s);
-    MVS_RC(launch_wgrad(d_x, cin, d_dz, cout, batch, height, width, d_dw, d_db, st));
+    MVS_RC(launch_wgrad(d_x, cin, d_dz, cout, batch, height, width, d_dw, d_db, d_err, st, tensor_cores != 0));
     if (d_dx)
         MVS_RC(launch_conv(d_dz, cout, d_wpack + s, nullptr, mask_x ? d_x : nullptr, d_dx, cin, batch, height, width,
                            0, d_err, st));

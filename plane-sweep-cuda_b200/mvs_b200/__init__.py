@@ -77,6 +77,18 @@ class BoxSceneDesc(C.Structure):
                 ("offsets", (C.c_double * 3) * 8)]
 
 
+class BatchFrameDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("n_views", C.c_int32), ("n_planes", C.c_int32),
+                ("window", C.c_int32), ("std_threshold", C.c_float), ("zfar", C.c_float), ("d_ref", C.c_void_p),
+                ("d_srcs", C.c_void_p), ("d_depths", C.c_void_p), ("h_K9", C.POINTER(C.c_double)),
+                ("h_Rrel", C.POINTER(C.c_double)), ("h_trel", C.POINTER(C.c_double)), ("d_depth", C.c_void_p),
+                ("d_labels", C.c_void_p), ("d_best", C.c_void_p)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("planes_per_chunk", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32)]
+
+
 def _sig(name, res, *args):
     f = getattr(_L, name)
     f.restype = res
@@ -113,7 +125,15 @@ _sig("mvs_unet_check", C.c_int, _VP, _VP)
 _sig("mvs_conv3x3_forward", C.c_int, _VP, C.c_int32, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
      C.c_int32, _VP, _VP, _VP, _VP)
 _sig("mvs_conv3x3_backward", C.c_int, _VP, C.c_int32, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-     C.c_int32, _VP, _VP, _VP, _VP, _VP, _VP)
+     C.c_int32, _VP, _VP, _VP, _VP, _VP, C.c_int32, _VP)
+_sig("mvs_batch_create", C.c_int, C.POINTER(_VP), C.POINTER(BatchFrameDesc), C.c_int32, C.c_int32,
+     C.POINTER(BatchTuning))
+_sig("mvs_batch_destroy", C.c_int, _VP)
+_sig("mvs_batch_get_tuning", C.c_int, _VP, C.POINTER(BatchTuning))
+_sig("mvs_batch_set_poses", C.c_int, _VP, _D, _D, _VP)
+_sig("mvs_batch_run", C.c_int, _VP, _VP)
+_sig("mvs_batch_frame_latency_ms", C.c_int, _VP, _F, _VP)
+_sig("mvs_batch_work_items", C.c_int64, _VP)
 _sig("mvs_tvl1_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32)
 _sig("mvs_tvl1_denoise", C.c_int, C.c_int32, C.c_int32, _VP, _VP, C.c_float, C.c_float, C.POINTER(TVL1Params),
      _VP, C.c_size_t, _VP)
@@ -325,6 +345,75 @@ def compute3d(depth, invK9, Rr9, t3, X, Y, Z, stream=None):
 
 
 # ---------------------------------------------------------------------------
+# batched frames
+# ---------------------------------------------------------------------------
+
+BATCH_ORDER_FRAME, BATCH_ORDER_LARGEST_FIRST, BATCH_ORDER_INTERLEAVED = 0, 1, 2
+
+
+class Batch:
+    """Handle on mvs_batch: many frames swept (aggregated mode) in one graph launch.
+
+    ``frames``: dicts with ``ref`` (H, W), ``srcs`` (V, H, W), ``depths`` (P)
+    CUDA float32 tensors, ``K1`` (3x3, 1-based), ``rel`` (list of (R, t) per
+    view), ``window``, ``zfar``, optional ``std_threshold`` and the output
+    tensors ``depth`` (H, W) and optional ``labels`` (int32) / ``best``.
+    ``tuning``: None (autotune) or (planes_per_chunk, ctas_per_sm, order)."""
+
+    def __init__(self, frames, moments=MOMENTS_COMPENSATED, tuning=None):
+        descs = (BatchFrameDesc * len(frames))()
+        keep = []
+        for d, f in zip(descs, frames):
+            H, W = f["ref"].shape
+            V = f["srcs"].shape[0]
+            K = np.ascontiguousarray(f["K1"], np.float64).reshape(9)
+            R = np.ascontiguousarray(np.stack([np.asarray(r, np.float64).reshape(9) for r, _ in f["rel"]]))
+            t = np.ascontiguousarray(np.stack([np.asarray(tt, np.float64).reshape(3) for _, tt in f["rel"]]))
+            keep += [K, R, t]
+            d.width, d.height, d.n_views, d.n_planes, d.window = W, H, V, f["depths"].numel(), f["window"]
+            d.std_threshold = f.get("std_threshold", 1e-4)
+            d.zfar = f["zfar"]
+            d.d_ref, d.d_srcs, d.d_depths = (x.data_ptr() for x in (f["ref"], f["srcs"], f["depths"]))
+            d.h_K9, d.h_Rrel, d.h_trel = (a.ctypes.data_as(_D) for a in (K, R, t))
+            d.d_depth = f["depth"].data_ptr()
+            d.d_labels = f["labels"].data_ptr() if f.get("labels") is not None else None
+            d.d_best = f["best"].data_ptr() if f.get("best") is not None else None
+        tn = None
+        if tuning is not None:
+            tn = BatchTuning(*tuning)
+        h = _VP()
+        check(_L.mvs_batch_create(C.byref(h), descs, len(frames), moments, None if tn is None else C.byref(tn)))
+        self._h = h
+        self.n = len(frames)
+
+    def close(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.mvs_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def tuning(self):
+        t = BatchTuning()
+        check(_L.mvs_batch_get_tuning(self._h, C.byref(t)))
+        return (t.planes_per_chunk, t.ctas_per_sm, t.order)
+
+    @property
+    def work_items(self):
+        return int(_L.mvs_batch_work_items(self._h))
+
+    def run(self, stream=None):
+        check(_L.mvs_batch_run(self._h, _stream(stream)))
+
+    def latencies_ms(self, stream=None):
+        out = np.empty(self.n, np.float32)
+        check(_L.mvs_batch_frame_latency_ms(self._h, out.ctypes.data_as(_F), _stream(stream)))
+        return out
+
+
+# ---------------------------------------------------------------------------
 # TGV2 warm-start network
 # ---------------------------------------------------------------------------
 
@@ -420,11 +509,11 @@ def conv3x3_forward(x, w, bias, relu, out, wpack, err, stream=None):
                                  _ptr(err), _stream(stream)))
 
 
-def conv3x3_backward(x, w, dz, mask_x, dx, dw, db, wpack, err, stream=None):
+def conv3x3_backward(x, w, dz, mask_x, dx, dw, db, wpack, err, tensor_cores=True, stream=None):
     B, H, W, cin = x.shape
     cout = w.shape[0]
     check(_L.mvs_conv3x3_backward(_ptr(x), cin, _ptr(w), _ptr(dz), cout, B, H, W, int(mask_x), _ptr(dx), _ptr(dw),
-                                  _ptr(db), _ptr(wpack), _ptr(err), _stream(stream)))
+                                  _ptr(db), _ptr(wpack), _ptr(err), int(tensor_cores), _stream(stream)))
 
 
 # ---------------------------------------------------------------------------

@@ -428,3 +428,51 @@ def fusion_sequence(seed: int, n_maps: int, width: int, height: int,
     half = cube / 2.0
     return FusionInput(depths, cams, np.array([-half, -1.5, -2.5]),
                        np.array([half, -1.5 + cube, 2.5]))
+
+
+# ---------------------------------------------------------------------------
+# batched uneven frames
+# ---------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class BatchFrameSpec:
+    kind: str          # "room320", "room640", "street"
+    seed: int
+    width: int
+    height: int
+    K: np.ndarray      # 0-based
+    n_src: int
+    n_planes: int
+    window: int
+    znear: float
+    zfar: float
+    baseline: tuple
+    rot_deg: float
+    scene: str
+
+
+def batch_workload(seed: int = 4, n: int = 48) -> list:
+    """Mixed frames: 320x240 and 640x480 box rooms and 1242x375 street frames
+    (KITTI-like intrinsics fx = 721.5, cx = 609.6, cy = 172.9), 64-256
+    inverse-depth planes, 4-8 source views and 5x5 to 11x11 windows, drawn
+    from `seed`."""
+    rng = np.random.default_rng(seed)
+    kinds = ("room320", "room640", "street")
+    out = []
+    for i in range(n):
+        kind = kinds[i % 3] if i < 3 else kinds[int(rng.integers(0, 3))]
+        P = int(rng.choice([64, 96, 128, 160, 192, 224, 256]))
+        V = int(rng.integers(4, 9))
+        win = int(rng.choice([5, 7, 9, 11]))
+        s = seed * 1000 + i
+        if kind == "room320":
+            spec = BatchFrameSpec(kind, s, 320, 240, intrinsics(240.0, 240.0, 160.0, 120.0), V, P, win, 0.5, 5.0,
+                                  (0.05, 0.05), 2.0, "room")
+        elif kind == "room640":
+            spec = BatchFrameSpec(kind, s, 640, 480, intrinsics(481.2, 481.2, 319.5, 239.5), V, P, win, 0.4, 8.0,
+                                  (0.02, 0.10), 2.0, "room")
+        else:
+            spec = BatchFrameSpec(kind, s, 1242, 375, intrinsics(721.5, 721.5, 609.6, 172.9), V, P, win, 2.0, 80.0,
+                                  (0.05, 0.5), 1.0, "street")
+        out.append(spec)
+    return out

@@ -250,23 +250,37 @@ def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=WARM_DU
         torch.cuda.synchronize()
         ms_w = a.elapsed_time(b)
         err_w = float((u - fr.depth_gt).abs().median())
-        # energy of the raw prediction and iterations to reach the plain energy
+        # energy of the raw prediction, and the iterations (0, 10, 20, ...) and
+        # device time (network included) the warm start needs to get below the
+        # plain run's final energy
+        a, b = ev(), ev()
+        a.record()
         pu, pv = ws.predict(wta[None], cost[None], fr.ref[None])
+        b.record()
+        torch.cuda.synchronize()
+        ms_net = a.elapsed_time(b)
         u.copy_(pu)
         v.copy_(pv)
         _, e0 = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=0), cams=cams)
-        n_reach = None
-        for n in (range(10, prm.max_iters + 1, 10) if reach else ()):
+        n_reach, ms_reach = None, None
+        if reach and e0 <= e_p:
+            n_reach, ms_reach = 0, ms_net
+        for n in (range(10, prm.max_iters + 1, 10) if reach and n_reach is None else ()):
+            a, b = ev(), ev()
+            a.record()
+            pu, pv = ws.predict(wta[None], cost[None], fr.ref[None])
             u.copy_(pu)
             v.copy_(pv)
             _, e = pipe.tgv(fr, wta, u, v, tgv_params(tol=0.0, max_iters=n), dual_sigma=dual_sigma,
                             dual_sigma_r=dual_sigma_r, cams=cams)
+            b.record()
+            torch.cuda.synchronize()
             if e <= e_p:
-                n_reach = n
+                n_reach, ms_reach = n, a.elapsed_time(b)
                 break
         rows.append(dict(seed=int(s), plain_ms=ms_p, plain_iters=it_p, plain_energy=e_p, plain_err=err_p,
                          warm_ms=ms_w, warm_iters=it_w, warm_energy=e_w, warm_err=err_w, start_energy=e0,
-                         warm_iters_to_plain_energy=n_reach))
+                         network_ms=ms_net, warm_iters_to_plain_energy=n_reach, warm_ms_to_plain_energy=ms_reach))
         if log:
             log(rows[-1])
     return rows

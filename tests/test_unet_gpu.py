@@ -69,6 +69,11 @@ def test_conv3x3_forward_and_backward(cuda, cin, cout):
                 U.conv3x3_backward(xn, np.abs(wn), np.abs(dzn))[0])
     assert _rel(dw.cpu().numpy().reshape(cout, cin, 9), rdw) < 1e-5
     assert _rel(db.cpu().numpy(), rdb) < 1e-5
+    # the CUDA-core formulation of the weight gradient agrees too
+    dw2 = torch.zeros_like(dw)
+    M.conv3x3_backward(x, w, dz.contiguous(), True, None, dw2, None, wpack, err, tensor_cores=False)
+    torch.cuda.synchronize()
+    assert _rel(dw2.cpu().numpy().reshape(cout, cin, 9), rdw) < 1e-5
 
 
 def _net_inputs(rng, B, H, W):

@@ -22,6 +22,10 @@ def test_warm_start_beats_plain_tgv2(cuda):
         assert r["warm_energy"] <= r["plain_energy"] * 1.005, r
         assert r["warm_iters_to_plain_energy"] is not None, r
         assert r["warm_err"] <= r["plain_err"] * 1.2, r
+    # the network's prediction alone is already within a few percent of (often
+    # below) the plain run's final energy; the winner-take-all start of the
+    # plain run sits tens of percent above it
+    assert np.median([r["start_energy"] / r["plain_energy"] for r in rows]) < 1.10
     reach = np.median([r["warm_iters_to_plain_energy"] for r in rows])
     plain_it = np.median([r["plain_iters"] for r in rows])
     assert reach * 3 <= plain_it, (reach, plain_it)
