@@ -38,6 +38,16 @@ import numpy as np  # noqa: E402
 
 METRIC = "Mpix·planes/s NCC sweep; ms/frame to TGV2 energy tol, warm-start vs plain"
 UNIT = "Mpix*planes/s"
+# per-launch DRAM traffic (bytes) of the dominant kernels, from one `ncu --set full` capture each
+# of `python bench.py --steps 2 --warmup 3 --tgv-steps 1 --no-cpu-baseline --no-batch
+# --no-warm-start --no-fusion` (one launch, dram__bytes_read.sum + dram__bytes_write.sum)
+NCU_TRAFFIC = {"sweep_aggregated_kernel": 13.586944e6 + 105.113856e6,
+               "wta_volume_kernel": 157.294336e6 + 3.661312e6,
+               "tgv2_iteration_kernel": 47.94624e6 + 0.278016e6}
+# algorithmic FP32 operations per (pixel, plane, view) evaluation of the fused sweep: homography
+# 15 (kernels.cu:31-44), bilinear 8 (kernels.cu:4-29), three running window moments 14
+# (kernels.cu:187-235), NCC 10 (kernels.cu:46-64), running best 3 (kernels.cu:66-82)
+SWEEP_OPS_PER_EVAL = 50
 W, H, V, P, WIN = 640, 480, 8, 256, 9
 SEED = 2
 
@@ -484,19 +494,30 @@ def main():
     ps.close()
 
     hbm, peak_kind = peaks()
+    # TGV2 iteration: 8 (8 + V) bytes of state read and written plus 4 (4 + 2V) bytes of constants
+    # per pixel (u, v, p, q, r_i; T, u0, It_i, Iu_i): 208 B at V = 8
+    tgv_roofline = None
+    if tgv_ms:
+        it_ms = tgv_ms_frame / max(tgv_iters, 1)
+        tb = (8 * (8 + V) + 4 * (4 + 2 * V)) * W * H
+        tgv_roofline = {"bound": "hbm", "kernel": "iteration_kernel<8>", "achieved": tb / (it_ms / 1e3) / 1e9,
+                        "peak": hbm, "unit": "GB/s", "frac": tb / (it_ms / 1e3) / 1e9 / hbm,
+                        "bytes_per_iteration": tb, "ms_per_iteration_incl_energy_checks": it_ms,
+                        "traffic": NCU_TRAFFIC["tgv2_iteration_kernel"]}
     sweep_s = statistics.median(sweep_ms) / 1e3
     # algorithmic bytes of the sweep kernel per launch: reference + 8 sources read once,
     # BF16 cost volume written once, WTA partials written once
     alg_bytes = (1 + V) * W * H * 4 + P * W * H * 2 + W * H * 8
     achieved = alg_bytes / sweep_s / 1e9
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        try:
-            traffic = json.loads(tfile.read_text()).get("sweep_aggregated_kernel")
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) of one launch of each kernel in an `ncu --set full` capture of
+    # this workload (one launch, L2 cold): the sweep's cost-volume writes partly stay in L2
+    traffic = NCU_TRAFFIC.get("sweep_aggregated_kernel")
     wta_bytes = P * W * H * 2 + W * H * (4 + 4 + 4) + P * 4
+    # FP32 roof of the sweep: SWEEP_OPS_PER_EVAL algorithmic FP32 operations per (pixel, plane,
+    # view) evaluation against one FP32 operation per lane per clock
+    sm_mhz = (clocks.summary() or {}).get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * sm_mhz * 1e6
+    fp32_achieved = evals * SWEEP_OPS_PER_EVAL / sweep_s
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -510,9 +531,14 @@ def main():
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                      "note": "the fused sweep is FP32/shared-memory issue bound; its HBM fraction is small by design",
                      "ms_per_launch": sweep_s * 1e3},
+        "fp32_roofline": {"bound": "fp32 issue", "kernel": "sweep_aggregated_kernel",
+                          "ops_per_eval": SWEEP_OPS_PER_EVAL, "achieved": fp32_achieved / 1e12,
+                          "peak": fp32_peak / 1e12, "unit": "T FP32 ops/s", "frac": fp32_achieved / fp32_peak,
+                          "peak_kind": "148 SMs x 128 FP32 lanes x max SM clock"},
         "wta_volume_roofline": {"bound": "hbm", "achieved": wta_bytes / (wta_ms / 1e3) / 1e9, "peak": hbm,
                                 "unit": "GB/s", "frac": wta_bytes / (wta_ms / 1e3) / 1e9 / hbm,
-                                "ms_per_launch": wta_ms},
+                                "ms_per_launch": wta_ms, "traffic": NCU_TRAFFIC.get("wta_volume_kernel")},
+        "tgv2_roofline": tgv_roofline,
         "tgv2": {"ms_per_frame_plain": tgv_ms_frame, "iterations": tgv_iters, "energy": tgv_e,
                  "tol": 1e-4, "cap": 500, "start": "WTA depth",
                  "ms_per_frame_warm_start": warm["ms_per_frame"] if warm else None, "warm_start": warm},

@@ -298,9 +298,39 @@ def main(argv=None):
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--norm", type=float, nargs=7, default=None)
     t.add_argument("--out", default=str(WEIGHTS))
+    tm = sub.add_parser("timing", help="device time of the network's forward pass and training step")
+    tm.add_argument("--batch", type=int, default=4)
+    tm.add_argument("--reps", type=int, default=10)
     a = ap.parse_args(argv)
     import mvs_b200 as M
     cfg = FrameConfig()
+    if a.cmd == "timing":
+        import torch
+        dev = torch.device("cuda")
+        B, H, W = a.batch, cfg.height, cfg.width
+        net = M.Unet(B, H, W)
+        net.init_params(0)
+        g = torch.Generator(device=dev).manual_seed(0)
+        args = [torch.rand((B, H, W), device=dev, generator=g) * 4 + 0.5, torch.rand((B, H, W), device=dev, generator=g),
+                torch.rand((B, H, W), device=dev, generator=g) * 255, torch.rand((B, H, W), device=dev, generator=g) * 4 + 0.5,
+                torch.rand((B, 2, H, W), device=dev, generator=g) * 0.01]
+        u = torch.empty((B, H, W), device=dev)
+        v = torch.empty((B, 2, H, W), device=dev)
+        res = {}
+        for name, fn in (("forward", lambda: net.forward(args[0], args[1], args[2], u, v)),
+                         ("train_step", lambda: net.train_step(*args, 1e-4))):
+            for _ in range(3):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(a.reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            res[name + "_ms"] = e0.elapsed_time(e1) / a.reps
+        net.check()
+        print(dict(batch=B, height=H, width=W, **res))
+        return
     norm = tuple(a.norm) if a.norm else M.UNET_DEFAULT_NORM
     data = make_dataset(range(a.first_seed, a.first_seed + a.scenes), cfg, a.target_iters, log=print)
     params, losses = train(data, a.steps, a.batch, a.lr, norm=norm, log=print)
