@@ -351,7 +351,7 @@ typedef struct mvs_batch_frame {
 
 typedef struct mvs_batch_tuning {
     int32_t planes_per_chunk;   /* 0: whole plane range per item */
-    int32_t ctas_per_sm;        /* persistent CTAs per SM (1 or 2) */
+    int32_t ctas_per_sm;        /* persistent CTAs per SM (1..3) */
     int32_t order;              /* MVS_BATCH_ORDER_* */
 } mvs_batch_tuning;
 

@@ -70,7 +70,7 @@ int validate(const mvs_batch_frame &f, int i)
     if (f.width < 16 || f.height < 16) return set_error(MVS_ERR_ARG, "frame %d: size %dx%d", i, f.width, f.height);
     if (f.n_views < 1 || f.n_views > kBatchMaxViews)
         return set_error(MVS_ERR_ARG, "frame %d: 1..%d views", i, kBatchMaxViews);
-    if (f.n_planes < 1) return set_error(MVS_ERR_ARG, "frame %d: no planes", i);
+    if (f.n_planes < 1 || f.n_planes > 65535) return set_error(MVS_ERR_ARG, "frame %d: 1..65535 planes", i);
     if (f.window < 3 || f.window > 15 || f.window % 2 == 0)
         return set_error(MVS_ERR_ARG, "frame %d: window %d (odd, 3..15)", i, f.window);
     if (f.width < f.window || f.height < f.window) return set_error(MVS_ERR_ARG, "frame %d: narrower than its window", i);
@@ -218,7 +218,7 @@ int run_timed(mvs_batch *b, cudaStream_t st, float *ms)
 int autotune(mvs_batch *b, mvs_batch_tuning *best)
 {
     const int chunks[] = {16, 32, 64, 0};
-    const int ctas[] = {1, 2};
+    const int ctas[] = {1, 2, 3};
     const int orders[] = {MVS_BATCH_ORDER_FRAME, MVS_BATCH_ORDER_LARGEST_FIRST, MVS_BATCH_ORDER_INTERLEAVED};
     float best_ms = 1e30f;
     for (int c : chunks)

@@ -141,6 +141,9 @@ static int check_sweep_desc(const mvs_sweep_desc *d)
     if (d->mode != MVS_SWEEP_PER_VIEW && d->mode != MVS_SWEEP_AGGREGATED)
         return set_error(MVS_ERR_ARG, "unknown sweep mode %d", d->mode);
     if ((long long)d->width * d->height > (1ll << 30)) return set_error(MVS_ERR_ARG, "image too large");
+    // the aggregated mode keeps the running best as (bf16 cost << 16 | plane)
+    if (d->mode == MVS_SWEEP_AGGREGATED && d->n_planes > 65535)
+        return set_error(MVS_ERR_ARG, "aggregated mode: at most 65535 planes (%d)", d->n_planes);
     return MVS_OK;
 }
 

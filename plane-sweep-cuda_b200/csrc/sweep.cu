@@ -473,42 +473,196 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
 }
 
 // ---- aggregated mode: cost = 1 - mean NCC over views, BF16 WTA -------------------
-// One CTA's work: tile (tx, ty) of the frame, planes of `chunk`.
+//
+// The per-CTA state that the per-view kernel keeps in registers -- the
+// reference column of pass A1, the region row coordinates of pass A0 and the
+// reference moments of pass B -- lives in shared memory here (AggSmem), and
+// the running best cost and plane are one 32-bit key (bf16 cost bits << 16 |
+// plane: non-negative bf16 values order like integers, and equal costs keep
+// the earlier plane), so the kernel fits three CTAs per SM.  The arithmetic is
+// the per-view kernel's.
 
+struct __align__(16) AggSmem {
+    Smem S;
+    float Rf[TH + 16][RWMAX];   // reference region (shifted in the compensated mode)
+    float Yc[TH + 16];          // region row coordinates (1-based, mirrored)
+    float RM[TH][RWMAX];        // reference window sums / means per output pixel
+    float RS[TH][RWMAX];        // reference n^2 var / std per output pixel
+};
+
+// pass A0 with the row coordinates from shared memory
 template <int WIN, int MOM>
-__device__ __forceinline__ void aggregated_tile(Smem &S, const SweepArgs &a, int tx, int ty, int chunk)
+__device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h,
+                                             const float *Hm, float X, const float *Yc)
 {
     using G = Geo<WIN>;
+    constexpr int CELLS = A0Cells<WIN>::CELLS;
+    constexpr int BATCH = 4;
+    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
+    if (rx >= G::RW) return;
+    const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
+    const float wm1 = (float)(w - 1), hm1 = (float)(h - 1);
+#pragma unroll
+    for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
+        float fa[BATCH], fb[BATCH];
+        int off[BATCH];
+        bool ok[BATCH];
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const int k = k0 + j;
+            ok[j] = false;
+            off[j] = 0;
+            fa[j] = fb[j] = 0.f;
+            if (k < CELLS && rb + 4 * k < G::RH) {
+                const float Y = Yc[rb + 4 * k];
+                float xs, ys;
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
+                    const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
+                    const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
+                    xs = q0 / q2 - 1.f;
+                    ys = q1 / q2 - 1.f;
+                } else {
+                    const float q0 = fmaf(Hm[1], Y, a0), q1 = fmaf(Hm[4], Y, a1), q2 = fmaf(Hm[7], Y, a2);
+                    float rz;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rz) : "f"(q2));
+                    xs = fmaf(q0, rz, -1.f);
+                    ys = fmaf(q1, rz, -1.f);
+                }
+                const float fx = floorf(xs), fy = floorf(ys);
+                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= wm1 && fy + 1.f <= hm1;
+                if (ok[j]) {
+                    fa[j] = xs - fx;
+                    fb[j] = ys - fy;
+                    off[j] = (int)fy * w + (int)fx;
+                }
+            }
+        }
+        float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
+            if (ok[j]) {
+                const float *r0 = src + off[j];
+                d00[j] = ldg(r0);
+                d01[j] = ldg(r0 + 1);
+                d10[j] = ldg(r0 + w);
+                d11[j] = ldg(r0 + w + 1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const int k = k0 + j;
+            if (k >= CELLS || rb + 4 * k >= G::RH) continue;
+            float v = 0.f;
+            if (ok[j]) {
+                const float a = fa[j], b = fb[j];
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    const float t1 = a * d01[j] + (1 - a) * d00[j];
+                    const float t2 = a * d11[j] + (1 - a) * d10[j];
+                    v = b * t2 + (1 - b) * t1;
+                } else {
+                    const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
+                    const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
+                    v = fmaf(b, t2 - t1, t1);
+                }
+            }
+            Wt[rb + 4 * k][rx] = v;
+        }
+    }
+}
+
+// pass A1 with the reference column read from shared memory
+template <int WIN, int MOM>
+__device__ __forceinline__ void pass_a1_rows(float (*Wt)[RWMAX], float (*CS)[TH][CSP], float (*Rf)[RWMAX],
+                                             float shift)
+{
+    using G = Geo<WIN>;
+    const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+    if (c >= G::RW) return;
+    float wv[G::SROWS];
+#pragma unroll
+    for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[8 * s + i][c];
+    if (MOM == MVS_MOMENTS_REFERENCE) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float s1 = 0.f, s2 = 0.f, s12 = 0.f;
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) {
+                const float x = wv[k + i];
+                s1 = s1 + x;
+                s2 = s2 + x * x;
+                s12 = s12 + Rf[8 * s + k + i][c] * x;
+            }
+            s1 = s1 / (float)WIN;
+            s2 = s2 / (float)WIN;
+            s12 = s12 / (float)WIN;
+            CS[0][8 * s + k][c] = s1;
+            CS[1][8 * s + k][c] = s2;
+            CS[2][8 * s + k][c] = s12;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < G::SROWS; ++i) wv[i] -= shift;
+        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) {
+            s1 += wv[i];
+            s2 = fmaf(wv[i], wv[i], s2);
+            s12 = fmaf(Rf[8 * s + i][c], wv[i], s12);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k > 0) {
+                const float xn = wv[k + WIN - 1], xo = wv[k - 1];
+                s1 = (s1 + xn) - xo;
+                s2 = fmaf(-xo, xo, fmaf(xn, xn, s2));
+                s12 = fmaf(-Rf[8 * s + k - 1][c], xo, fmaf(Rf[8 * s + k + WIN - 1][c], xn, s12));
+            }
+            CS[0][8 * s + k][c] = s1;
+            CS[1][8 * s + k][c] = s2;
+            CS[2][8 * s + k][c] = s12;
+        }
+    }
+}
+
+// One CTA's work: tile (tx, ty) of the frame, planes of `chunk`.
+template <int WIN, int MOM>
+__device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, int tx, int ty, int chunk)
+{
+    using G = Geo<WIN>;
+    Smem &S = A.S;
     const int x0 = tx * G::TW, y0 = ty * TH;
     const int w = a.w, h = a.h;
     const size_t n = (size_t)w * h;
 
     load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    for (int i = threadIdx.x; i < G::RH; i += THREADS) A.Yc[i] = (float)(mirror_idx(y0 - G::R + i, h) + 1);
     __syncthreads();
     const float shift = tile_shift<WIN, MOM>(S);
-    float refcol[G::SROWS];
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
+        A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+    }
     {
-        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
+        float rm[G::RUN], rs[G::RUN];
+        ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+        const int yy = threadIdx.x >> 3, g = threadIdx.x & 7;
 #pragma unroll
-        for (int i = 0; i < G::SROWS; ++i) {
-            const float r = (c < G::RW) ? S.Wt[8 * s + i][c] : 0.f;
-            refcol[i] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+        for (int j = 0; j < G::RUN; ++j) {
+            A.RM[yy][g * G::RUN + j] = rm[j];
+            A.RS[yy][g * G::RUN + j] = rs[j];
         }
     }
-    float rm[G::RUN], rs[G::RUN];
-    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
-    float Xcol, Ycol[A0Cells<WIN>::CELLS];
-    a0_setup<WIN>(w, h, x0, y0, Xcol, Ycol);
+    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x & 63), w) + 1);
 
     const int y = y0 + (threadIdx.x >> 3);
     const int xb = x0 + (threadIdx.x & 7) * G::RUN;
-    float bestc[G::RUN];
-    int lab[G::RUN];
+    const int ly = threadIdx.x >> 3, lx = (threadIdx.x & 7) * G::RUN;
+    uint32_t best[G::RUN];   // (bf16 cost bits << 16) | plane
 #pragma unroll
-    for (int j = 0; j < G::RUN; ++j) {
-        bestc[j] = 3.f;
-        lab[j] = -1;
-    }
+    for (int j = 0; j < G::RUN; ++j) best[j] = 0xffffffffu;
     const float invV = 1.f / (float)a.V;
     const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
     for (int p = p0; p < p1; ++p) {
@@ -521,16 +675,17 @@ __device__ __forceinline__ void aggregated_tile(Smem &S, const SweepArgs &a, int
             float Hm[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-            pass_a0<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, Hm, Xcol, Ycol);
+            pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, Hm, Xcol, A.Yc);
             __syncthreads();
-            pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
+            pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf, shift);
             __syncthreads();
             float s1[G::RUN], s2[G::RUN], s12[G::RUN];
             row_sums<WIN, MOM>(S.CS, 0, s1);
             row_sums<WIN, MOM>(S.CS, 1, s2);
             row_sums<WIN, MOM>(S.CS, 2, s12);
 #pragma unroll
-            for (int j = 0; j < G::RUN; ++j) acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
+            for (int j = 0; j < G::RUN; ++j)
+                acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], A.RM[ly][lx + j], A.RS[ly][lx + j], a.stdthresh);
         }
 #pragma unroll
         for (int j = 0; j < G::RUN; ++j) {
@@ -539,13 +694,9 @@ __device__ __forceinline__ void aggregated_tile(Smem &S, const SweepArgs &a, int
             float cf = fmaf(-acc[j], invV, 1.f);
             cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
             const uint16_t cb = f2bf(cf);
-            const float c = bf2f(cb);
             const int x = xb + j;
             if (a.cost && y < h && x < w) a.cost[(size_t)p * n + (size_t)y * w + x] = cb;
-            if (c < bestc[j]) {
-                bestc[j] = c;
-                lab[j] = p;
-            }
+            best[j] = min(best[j], ((uint32_t)cb << 16) | (uint32_t)p);
         }
     }
     if (y >= h) return;
@@ -555,20 +706,22 @@ __device__ __forceinline__ void aggregated_tile(Smem &S, const SweepArgs &a, int
         if (x >= w) break;
         // (cost bits << 32) | plane: a 64-bit min keeps the lowest cost and,
         // among equal costs, the earliest plane (costs are >= 0).
-        const unsigned long long key = lab[j] < 0 ? ~0ull
-            : ((unsigned long long)__float_as_uint(bestc[j]) << 32) | (unsigned)lab[j];
+        const bool any = best[j] != 0xffffffffu;
+        const unsigned long long key = !any ? ~0ull
+            : ((unsigned long long)__float_as_uint(bf2f((uint16_t)(best[j] >> 16))) << 32) | (best[j] & 0xffffu);
         unsigned long long *o = a.wta + (size_t)y * w + x;
         if (a.n_chunks == 1) *o = key;
-        else if (lab[j] >= 0) atomicMin(o, key);
+        else if (any) atomicMin(o, key);
     }
 }
 
-// grid: (tiles_x, tiles_y, n_chunks)
+// grid: (tiles_x, tiles_y, n_chunks); dynamic shared memory: sizeof(AggSmem)
 template <int WIN, int MOM>
-__global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_kernel(SweepArgs a)
+__global__ void __launch_bounds__(THREADS, 3) sweep_aggregated_kernel(SweepArgs a)
 {
-    __shared__ Smem S;
-    aggregated_tile<WIN, MOM>(S, a, blockIdx.x, blockIdx.y, blockIdx.z);
+    extern __shared__ __align__(16) unsigned char agg_smem[];
+    AggSmem &A = *reinterpret_cast<AggSmem *>(agg_smem);
+    aggregated_tile<WIN, MOM>(A, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---- epilogues ----------------------------------------------------------------------
@@ -728,11 +881,12 @@ __global__ void batch_start_kernel(unsigned int *next, unsigned long long *t_sta
 }
 
 template <int MOM>
-__global__ void __launch_bounds__(THREADS, 2) sweep_batch_kernel(const BatchFrameDev *__restrict__ frames,
+__global__ void __launch_bounds__(THREADS, 3) sweep_batch_kernel(const BatchFrameDev *__restrict__ frames,
                                                                   const uint4 *__restrict__ items, int n_items,
                                                                   unsigned int *next)
 {
-    __shared__ Smem S;
+    extern __shared__ __align__(16) unsigned char agg_smem[];
+    AggSmem &S = *reinterpret_cast<AggSmem *>(agg_smem);
     __shared__ int s_item, s_last;
     for (;;) {
         if (threadIdx.x == 0) s_item = (int)atomicAdd(next, 1u);
@@ -844,7 +998,12 @@ int launch_window(int win, const SweepArgs &a, int mode, void *stream)
         dim3 grid(ceil_div(a.w, Geo<WIN>::TW), ceil_div(a.h, TH),                                    \
                   mode == MVS_SWEEP_PER_VIEW ? a.V * a.n_chunks : a.n_chunks);                       \
         if (mode == MVS_SWEEP_PER_VIEW) sweep_view_kernel<WIN, MOM><<<grid, THREADS, 0, st>>>(a);   \
-        else sweep_aggregated_kernel<WIN, MOM><<<grid, THREADS, 0, st>>>(a);                        \
+        else {                                                                                       \
+            MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_aggregated_kernel<WIN, MOM>,                        \
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+                                              (int)sizeof(AggSmem)));                                    \
+            sweep_aggregated_kernel<WIN, MOM><<<grid, THREADS, sizeof(AggSmem), st>>>(a);              \
+        }                                                                                            \
         return check_launch("sweep kernel");                                                         \
     }
     switch (win) {
@@ -933,10 +1092,16 @@ int sweep_batch_launch(const BatchFrameDev *frames, const uint4 *items, int n_it
     cudaStream_t st = (cudaStream_t)stream;
     batch_start_kernel<<<1, 1, 0, st>>>(next, t_start);
     if (n_hom > 0) homography_batch_kernel<<<ceil_div(n_hom, 128), 128, 0, st>>>(cams, hom_offsets, n_frames);
-    if (moments == MVS_MOMENTS_REFERENCE)
-        sweep_batch_kernel<MVS_MOMENTS_REFERENCE><<<ctas, THREADS, 0, st>>>(frames, items, n_items, next);
-    else
-        sweep_batch_kernel<MVS_MOMENTS_COMPENSATED><<<ctas, THREADS, 0, st>>>(frames, items, n_items, next);
+    const int sm = (int)sizeof(AggSmem);
+    if (moments == MVS_MOMENTS_REFERENCE) {
+        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MVS_MOMENTS_REFERENCE>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        sweep_batch_kernel<MVS_MOMENTS_REFERENCE><<<ctas, THREADS, sm, st>>>(frames, items, n_items, next);
+    } else {
+        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MVS_MOMENTS_COMPENSATED>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        sweep_batch_kernel<MVS_MOMENTS_COMPENSATED><<<ctas, THREADS, sm, st>>>(frames, items, n_items, next);
+    }
     return check_launch("sweep batch");
 }
 

@@ -56,7 +56,7 @@ def _single(cuda, f):
 
 
 @pytest.mark.parametrize("tuning", [(8, 2, M.BATCH_ORDER_INTERLEAVED), (0, 1, M.BATCH_ORDER_FRAME),
-                                    (16, 2, M.BATCH_ORDER_LARGEST_FIRST)])
+                                    (16, 3, M.BATCH_ORDER_LARGEST_FIRST)])
 def test_batch_matches_single_frame_sweeps(cuda, tuning):
     import torch
     frames = _frames(cuda)
@@ -83,7 +83,7 @@ def test_batch_autotuner_picks_a_candidate(cuda):
     frames = _frames(cuda)
     b = M.Batch(frames, M.MOMENTS_COMPENSATED)
     ppc, ctas, order = b.tuning
-    assert ppc in (16, 32, 64, 0) and ctas in (1, 2) and order in (0, 1, 2)
+    assert ppc in (16, 32, 64, 0) and ctas in (1, 2, 3) and order in (0, 1, 2)
     b.run()
     torch.cuda.synchronize()
     d, lab, best = _single(cuda, frames[1])
