@@ -76,7 +76,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -86,7 +86,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def wait_first(self, timeout=5.0):
+        """Block until nvidia-smi has produced its first sample (or timeout)."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.01)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -96,10 +102,18 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, window=None):
+        """Median SM clock, max clock and active throttle reasons of the samples
+        taken inside `window` (host times), or of all samples when none fell
+        inside it (the window is then reported as the whole loaded run)."""
+        lines = [ln for t, ln in self.lines if window and window[0] <= t <= window[1]]
+        where = "timed region"
+        if not lines:
+            lines = [ln for _, ln in self.lines]
+            where = "whole bench run (all sections under load)"
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -113,7 +127,8 @@ class ClockSampler:
                     reasons.add(n)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "window": where, "interval_ms": 20}
 
 
 def make_frame(rank: int):
@@ -300,6 +315,10 @@ def main():
 
     launches_per_step = 4   # homography, sweep, sweep epilogue, WTA over the volume
 
+    # clocks and throttle reasons, sampled every 20 ms from before the warm-up to the end
+    clocks = ClockSampler(local).__enter__()
+    clocks.wait_first()
+
     # --- sweep: warm-up, then K timed steps (events per step; L2 flushed between steps) ---
     for _ in range(args.warmup):
         step()
@@ -308,17 +327,18 @@ def main():
     kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        for k in range(args.steps):
-            flush.zero_()
-            ev[k][0].record(stream)
-            M.sweep_homographies(desc, K1, rel, d_depths, d_H)
-            kev[k][0].record(stream)
-            M.sweep(desc, d_ref, d_srcs, d_H, d_depths, depth, None, None, cost, wsp)
-            kev[k][1].record(stream)
-            M.sweep_wta_volume(cost, d_depths, W * H, P, 8.0, depth, labels, best)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
+    t_timed0 = time.time()
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        M.sweep_homographies(desc, K1, rel, d_depths, d_H)
+        kev[k][0].record(stream)
+        M.sweep(desc, d_ref, d_srcs, d_H, d_depths, depth, None, None, cost, wsp)
+        kev[k][1].record(stream)
+        M.sweep_wta_volume(cost, d_depths, W * H, P, 8.0, depth, labels, best)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    timed_window = (t_timed0, time.time())
     dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     sweep_ms = [a.elapsed_time(b) for a, b in kev]
@@ -515,7 +535,9 @@ def main():
     wta_bytes = P * W * H * 2 + W * H * (4 + 4 + 4) + P * 4
     # FP32 roof of the sweep: SWEEP_OPS_PER_EVAL algorithmic FP32 operations per (pixel, plane,
     # view) evaluation against one FP32 operation per lane per clock
-    sm_mhz = (clocks.summary() or {}).get("sm_max_mhz") or 1965.0
+    clocks.__exit__(None, None, None)
+    clock_summary = clocks.summary(timed_window)
+    sm_mhz = (clock_summary or {}).get("sm_max_mhz") or 1965.0
     fp32_peak = 148 * 128 * sm_mhz * 1e6
     fp32_achieved = evals * SWEEP_OPS_PER_EVAL / sweep_s
     out = {
@@ -547,7 +569,7 @@ def main():
         "fusion": fusion,
         "batched": batched,
         "gpu_launches": launches_per_step * args.steps,
-        "clocks": clocks.summary(),
+        "clocks": clock_summary,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, secs, kind, cores, sample = cpu_reference_sample(fr, planes)

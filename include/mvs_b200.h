@@ -149,7 +149,12 @@ typedef struct mvs_tgv2_params {
                              checks inside one linearisation; 0 = fixed count */
     int32_t check_every;  /* iterations between energy evaluations (tol > 0) */
     int32_t max_iters;    /* extension: total cap (0 = warps * niters) */
+    int32_t iteration_kernel; /* MVS_TGV2_ITER_*: how the iterations run (same results) */
 } mvs_tgv2_params;
+
+#define MVS_TGV2_ITER_AUTO 0     /* one cooperative launch per linearisation with the state on
+                                    chip when the image fits one tile per SM, else as below */
+#define MVS_TGV2_ITER_LAUNCH 1   /* one fused launch per iteration, state in HBM/L2 */
 
 size_t mvs_tgv2_workspace_bytes(int32_t width, int32_t height, int32_t n_views);
 

@@ -36,7 +36,9 @@ static void clear_error() { g_err[0] = 0; }
 int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode);
 int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
                  float *depth, int32_t *labels, float *best, uint16_t *cost, unsigned long long *scratch,
-                 int n_chunks, void *stream);
+                 int n_chunks, void *stream, float4 *quad = nullptr);
+size_t sweep_scratch_bytes(const mvs_sweep_desc *d);
+size_t sweep_quad_bytes(const mvs_sweep_desc *d);
 int sweep_wta_volume(const uint16_t *cost, const float *depths, int n, int P, float zfar, float *depth,
                      int32_t *labels, float *best, void *stream);
 int sweep_homographies(const double *K, const double *invK, const double *Rrel, const double *trel,
@@ -150,9 +152,8 @@ static int check_sweep_desc(const mvs_sweep_desc *d)
 size_t mvs_sweep_workspace_bytes(const mvs_sweep_desc *d)
 {
     if (check_sweep_desc(d)) return 0;
-    const size_t n = (size_t)d->width * d->height;
-    return d->mode == MVS_SWEEP_PER_VIEW ? n * d->n_views * sizeof(unsigned long long)
-                                         : n * sizeof(unsigned long long);
+    // winner words, then (aggregated mode) the sources' 2x2 neighbourhoods
+    return (sweep_scratch_bytes(d) + 255) / 256 * 256 + sweep_quad_bytes(d);
 }
 
 int mvs_sweep_homographies(const mvs_sweep_desc *d, const double *K, const double *Rrel, const double *trel,
@@ -186,7 +187,9 @@ int mvs_sweep(const mvs_sweep_desc *d, const float *ref, const float *srcs, cons
     if (((uintptr_t)ws) & 7) return set_error(MVS_ERR_ARG, "workspace must be 8-byte aligned");
     if (d->mode == MVS_SWEEP_PER_VIEW && cost) return set_error(MVS_ERR_ARG, "cost volume is an aggregated-mode output");
     const int chunks = sweep_pick_chunks(d->window, d->width, d->height, d->n_views, d->n_planes, d->mode);
-    return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)ws, chunks, stream);
+    float4 *quad = sweep_quad_bytes(d) ? (float4 *)((char *)ws + (sweep_scratch_bytes(d) + 255) / 256 * 256) : nullptr;
+    return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)ws, chunks, stream,
+                        quad);
 }
 
 int mvs_sweep_wta_volume(const uint16_t *cost, const float *depths, int32_t n_pixels, int32_t n_planes, float zfar,

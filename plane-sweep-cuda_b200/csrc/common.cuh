@@ -64,6 +64,7 @@ struct BatchFrameDev {
     unsigned int *tile_left;      // [n_tiles] chunks still running
     unsigned int *frame_left;     // tiles still running
     unsigned long long *done_ns;  // completion time of the last launch
+    const float4 *quad;           // [V][w*h] 2x2 source neighbourhoods, or null
     int w, h, V, P, win, planes_per_chunk, n_chunks, tiles_x, n_tiles, tile_w;
     float stdthresh, zfar;
 };

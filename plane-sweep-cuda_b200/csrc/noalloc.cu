@@ -23,7 +23,8 @@ namespace mvs {
 int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode);
 int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
                  float *depth, int32_t *labels, float *best, uint16_t *cost, unsigned long long *scratch,
-                 int n_chunks, void *stream);
+                 int n_chunks, void *stream, float4 *quad);
+size_t sweep_scratch_bytes(const mvs_sweep_desc *d);
 
 // 32 MiB: 4 Mi 64-bit words, one per pixel and source view in the per-view
 // mode (a 640x480 frame with up to 13 views) or one per pixel in the
@@ -67,8 +68,10 @@ int mvs_sweep_noalloc(const mvs_sweep_desc *d, const float *ref, const float *sr
                       const float *depths, float *depth, int32_t *labels, float *best, uint16_t *cost, void *stream)
 {
     using namespace mvs;
-    const size_t need = mvs_sweep_workspace_bytes(d);   // validates d; 0 if invalid
-    if (need == 0) return MVS_ERR_ARG;
+    if (mvs_sweep_workspace_bytes(d) == 0) return MVS_ERR_ARG;   // validates d
+    // only the winner words: the fixed array holds no 2x2 source neighbourhoods
+    // (the kernel then gathers the four samples itself)
+    const size_t need = sweep_scratch_bytes(d);
     if (need > kNoAllocScratchBytes)
         return set_error(MVS_ERR_ARG,
                          "mvs_sweep_noalloc: this sweep needs %zu bytes of scratch, the fixed array holds %zu "
@@ -80,7 +83,7 @@ int mvs_sweep_noalloc(const mvs_sweep_desc *d, const float *ref, const float *sr
     if (int rc = scratch_address(&scratch)) return rc;
     const int chunks = sweep_pick_chunks(d->window, d->width, d->height, d->n_views, d->n_planes, d->mode);
     return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)scratch, chunks,
-                        stream);
+                        stream, nullptr);
 }
 
 }  // extern "C"

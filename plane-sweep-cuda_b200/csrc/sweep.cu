@@ -67,6 +67,7 @@ struct SweepArgs {
     unsigned long long *packed;   // PER_VIEW: [V][n] best (ncc bits << 32 | ~plane)
     unsigned long long *wta;      // AGGREGATED: [n] (cost bits << 32 | plane)
     uint16_t *cost;               // AGGREGATED: [P][n] bf16 or null
+    const float4 *quad;           // AGGREGATED: [V][n] 2x2 neighbourhoods of the sources, or null
 };
 
 // ---- pass A0: warp the region into shared memory ------------------------------
@@ -490,10 +491,31 @@ struct __align__(16) AggSmem {
     float RS[TH][RWMAX];        // reference n^2 var / std per output pixel
 };
 
-// pass A0 with the row coordinates from shared memory
+// Each source pixel's 2x2 bilinear neighbourhood (x, x+1 on rows y, y+1) as
+// one aligned 16-byte word, so that a warp sample is one load instead of four
+// (the values, and so the arithmetic, are unchanged).  Only x <= w-2, y <= h-2
+// are ever read; the last row and column hold zeros.
+__global__ void quad_kernel(const float *__restrict__ src, int V, int w, int h, float4 *__restrict__ quad)
+{
+    const size_t n = (size_t)w * h, total = n * V;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = i / n, k = i - v * n;
+        const int y = (int)(k / w), x = (int)(k - (size_t)y * w);
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (x < w - 1 && y < h - 1) {
+            const float *r = src + v * n + k;
+            q = make_float4(r[0], r[1], r[w], r[w + 1]);
+        }
+        quad[i] = q;
+    }
+}
+
+// pass A0 with the row coordinates from shared memory; `quad` (may be null)
+// holds the source's 2x2 neighbourhoods
 template <int WIN, int MOM>
-__device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h,
-                                             const float *Hm, float X, const float *Yc)
+__device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src,
+                                             const float4 *__restrict__ quad, int w, int h, const float *Hm, float X,
+                                             const float *Yc)
 {
     using G = Geo<WIN>;
     constexpr int CELLS = A0Cells<WIN>::CELLS;
@@ -539,15 +561,29 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
             }
         }
         float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
+        if (quad) {
 #pragma unroll
-        for (int j = 0; j < BATCH; ++j) {
-            d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
-            if (ok[j]) {
-                const float *r0 = src + off[j];
-                d00[j] = ldg(r0);
-                d01[j] = ldg(r0 + 1);
-                d10[j] = ldg(r0 + w);
-                d11[j] = ldg(r0 + w + 1);
+            for (int j = 0; j < BATCH; ++j) {
+                d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
+                if (ok[j]) {
+                    const float4 q = __ldg(quad + off[j]);
+                    d00[j] = q.x;
+                    d01[j] = q.y;
+                    d10[j] = q.z;
+                    d11[j] = q.w;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < BATCH; ++j) {
+                d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
+                if (ok[j]) {
+                    const float *r0 = src + off[j];
+                    d00[j] = ldg(r0);
+                    d01[j] = ldg(r0 + 1);
+                    d10[j] = ldg(r0 + w);
+                    d11[j] = ldg(r0 + w + 1);
+                }
             }
         }
 #pragma unroll
@@ -675,7 +711,8 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             float Hm[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-            pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, w, h, Hm, Xcol, A.Yc);
+            pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, a.quad ? a.quad + (size_t)view * n : nullptr, w, h,
+                                   Hm, Xcol, A.Yc);
             __syncthreads();
             pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf, shift);
             __syncthreads();
@@ -910,6 +947,7 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_batch_kernel(const BatchFram
         a.packed = nullptr;
         a.wta = f.wta;
         a.cost = nullptr;
+        a.quad = f.quad;
         const int tx = (int)item.y % f.tiles_x, ty = (int)item.y / f.tiles_x;
         switch (f.win) {
         case 3: aggregated_tile<3, MOM>(S, a, tx, ty, item.z); break;
@@ -1038,9 +1076,20 @@ int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode)
     return chunks;
 }
 
+size_t sweep_scratch_bytes(const mvs_sweep_desc *d)
+{
+    const size_t n = (size_t)d->width * d->height;
+    return (d->mode == MVS_SWEEP_PER_VIEW ? n * d->n_views : n) * sizeof(unsigned long long);
+}
+
+size_t sweep_quad_bytes(const mvs_sweep_desc *d)
+{
+    return d->mode == MVS_SWEEP_AGGREGATED ? (size_t)d->width * d->height * d->n_views * sizeof(float4) : 0;
+}
+
 int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
                  float *depth, int32_t *labels, float *best, uint16_t *cost, unsigned long long *scratch,
-                 int n_chunks, void *stream)
+                 int n_chunks, void *stream, float4 *quad)
 {
     cudaStream_t st = (cudaStream_t)stream;
     const int n = d->width * d->height;
@@ -1060,6 +1109,13 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     a.packed = nullptr;
     a.wta = nullptr;
     a.cost = nullptr;
+    a.quad = nullptr;
+    if (d->mode == MVS_SWEEP_AGGREGATED && quad) {
+        const size_t total = (size_t)n * d->n_views;
+        const size_t blocks = (total + 255) / 256 < (size_t)16 * kSMs ? (total + 255) / 256 : (size_t)16 * kSMs;
+        quad_kernel<<<(int)blocks, 256, 0, st>>>(srcs, d->n_views, d->width, d->height, quad);
+        a.quad = quad;
+    }
     if (d->mode == MVS_SWEEP_PER_VIEW) {
         a.packed = scratch;
         if (a.n_chunks > 1)

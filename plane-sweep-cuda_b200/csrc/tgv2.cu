@@ -199,6 +199,37 @@ struct IterBufs {
 // FP64 square root when s <= 1 (then the result is exactly 1).
 __device__ __forceinline__ double proj_norm(double s) { return s > 1.0 ? (double)fmaxf(1.f, (float)sqrt(s)) : 1.0; }
 
+// r / fmaxf(1, |r|) of TGV2_updateR (TGV2_kernels.cu:99-101) without the
+// division: |r| <= 1 divides by 1 and |r| > 1 divides r by its own magnitude,
+// exactly +-1 in IEEE arithmetic (NaN stays NaN, as in the division).
+__device__ __forceinline__ float proj_unit(float r) { return fabsf(r) > 1.f ? copysignf(1.f, r) : r; }
+
+// (float)(v / d) for the reference's projections with d = proj_norm(s): the
+// square root and the FP64 divisions sit behind real branches, so warps whose
+// projections are all the identity skip them.
+__device__ __forceinline__ void proj2(double s, double &a, double &b)
+{
+    if (s > 1.0) {
+        const double d = (double)fmaxf(1.f, (float)sqrt(s));
+        if (d != 1.0) {
+            a = a / d;
+            b = b / d;
+        }
+    }
+}
+
+__device__ __forceinline__ void proj3(double s, double &a, double &b, double &c)
+{
+    if (s > 1.0) {
+        const double d = (double)fmaxf(1.f, (float)sqrt(s));
+        if (d != 1.0) {
+            a = a / d;
+            b = b / d;
+            c = c / d;
+        }
+    }
+}
+
 // One full TGV2 iteration (planesweep.cpp:485-509).  The pixel's own operands
 // (r, It, Iu of every view, T, u, u0, v) are loaded before the shared-memory
 // phase so their latency overlaps the halo work.
@@ -264,24 +295,24 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
             const double xg = sU[ry][nx] - sU[ry][rx] - sVX[ry][rx];
             const double yg = sU[ny][rx] - sU[ry][rx] - sVY[ry][rx];
             const double c11 = b.T11[j], c12 = b.T12[j], c22 = b.T22[j];
-            const double dx = (double)b.Px_in[j] + (double)a1s * (c11 * xg + c12 * yg);
-            const double dy = (double)b.Py_in[j] + (double)a1s * (c12 * xg + c22 * yg);
-            const double d = proj_norm(dx * dx + dy * dy);
-            sPx[ry][rx] = (float)(d == 1.0 ? dx : dx / d);
-            sPy[ry][rx] = (float)(d == 1.0 ? dy : dy / d);
+            double dx = (double)b.Px_in[j] + (double)a1s * (c11 * xg + c12 * yg);
+            double dy = (double)b.Py_in[j] + (double)a1s * (c12 * xg + c22 * yg);
+            proj2(dx * dx + dy * dy, dx, dy);
+            sPx[ry][rx] = (float)dx;
+            sPy[ry][rx] = (float)dy;
         }
         {
             const float dx_u1x = sVX[ry][nx] - sVX[ry][rx];
             const float dy_u1x = sVX[ny][rx] - sVX[ry][rx];
             const float dx_u1y = sVY[ry][nx] - sVY[ry][rx];
             const float dy_u1y = sVY[ny][rx] - sVY[ry][rx];
-            const double dx = b.Qx_in[j] + a0s * dx_u1x;
-            const double dy = b.Qy_in[j] + a0s * dy_u1y;
-            const double dz = b.Qz_in[j] + a0s * (dy_u1x + dx_u1y) / 2.0f;
-            const double d = proj_norm(dx * dx + dy * dy + dz * dz + dz * dz);
-            sQx[ry][rx] = (float)(d == 1.0 ? dx : dx / d);
-            sQy[ry][rx] = (float)(d == 1.0 ? dy : dy / d);
-            sQz[ry][rx] = (float)(d == 1.0 ? dz : dz / d);
+            double dx = b.Qx_in[j] + a0s * dx_u1x;
+            double dy = b.Qy_in[j] + a0s * dy_u1y;
+            double dz = b.Qz_in[j] + a0s * (dy_u1x + dx_u1y) / 2.0f;
+            proj3(dx * dx + dy * dy + dz * dz + dz * dz, dx, dy, dz);
+            sQx[ry][rx] = (float)dx;
+            sQy[ry][rx] = (float)dy;
+            sQz[ry][rx] = (float)dz;
         }
     }
     __syncthreads();
@@ -296,8 +327,7 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
 #pragma unroll
     for (int v = 0; v < VMAX; ++v) {
         if (v < V) {
-            float r = rv[v] + sl * (itv[v] + du * iuv[v]);
-            r = r / fmaxf(1.f, fabsf(r));
+            const float r = proj_unit(rv[v] + sl * (itv[v] + du * iuv[v]));
             b.r[(size_t)v * n + i] = r;
             prodsum += r * iuv[v];
         }
@@ -434,10 +464,421 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
 
 constexpr int kEnergyBlocks = 2 * kSMs;
 
+// ---- persistent iteration: the state stays on chip -----------------------------------
+//
+// One CTA per SM owns a 64 x TH tile for a whole linearisation: u, v, their
+// over-relaxations, p, q, r of every view and the tensor T live in shared
+// memory (about 200 KB at 64 x 35 pixels and 8 views); u0, It and Iu stream
+// from L2.  An iteration is the fused kernel's arithmetic, statement for
+// statement, with one grid-wide barrier: every CTA publishes its edge pixels
+// (ubar, vbar on all four edges; p, q on the right column and bottom row) to a
+// double-buffered exchange array, waits at the barrier, and reads its halo.
+// Energy checks (every check_every iterations) evaluate the same energy as
+// energy_kernel: each CTA writes its partial sum, and after a second barrier
+// every CTA adds the partials in CTA order, so all reach the same stopping
+// decision without the host.  Co-residency comes from a cooperative launch;
+// each barrier wait gives up after 1 s (then every CTA leaves and the host
+// reports MVS_ERR_TIMEOUT).
+
+constexpr int PT_THREADS = 768;
+constexpr int PT_TW = 64;
+constexpr int PT_VMAX = 8;
+constexpr unsigned long long kBarrierNs = 1000000000ull;
+
+struct PersistResult {
+    int iters, energy_at, done, err;
+    double energy;
+};
+
+struct PersistBufs {
+    const float *T11, *T12, *T22, *u0, *It, *Iu;
+    float *u, *u1x, *u1y, *r;                  // state in / out
+    const float *ubar0, *u1xbar0, *u1ybar0;    // start of the over-relaxations
+    float *Px, *Py, *Qx, *Qy, *Qz;             // p, q in / out
+    float *exb[2], *exq[2], *exu;              // edge exchange: [3][n], [5][n], [3][n]
+    double *partial;                           // [grid]
+    unsigned int *bar;                         // count, generation, abort
+    PersistResult *res;
+    int w, h, V, tiles_x, th, niters, cap_left, check_every;
+    double tol;
+    float lambda, alpha0, alpha1, tau, sigma;
+    double dlambda, dalpha0, dalpha1;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier with a bounded wait; false (for every thread of the CTA)
+// if it gave up or another CTA did.  Thread 0 arrives with an acquire-release
+// add (after the CTA barrier, so the CTA's earlier writes are released with
+// it); the last to arrive resets the count and publishes the next generation
+// with a release store, the others poll it with acquire loads.
+__device__ bool grid_barrier(unsigned int *bar, unsigned int nblocks, unsigned int &gen)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned int g = gen;
+        unsigned int old;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+        if (old == nblocks - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(bar), "r"(0u) : "memory");
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(bar + 1), "r"(g + 1u) : "memory");
+        } else {
+            // the clock and the abort flag are looked at every 1024 polls
+            const unsigned long long t0 = now_ns();
+            unsigned int polls = 0;
+            while (ld_acquire_u32(&bar[1]) == g) {
+                if ((++polls & 1023u) == 0u &&
+                    (ld_acquire_u32(&bar[2]) != 0u || now_ns() - t0 > kBarrierNs)) {
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        if (!ok) atomicExch(&bar[2], 1u);
+        s_ok = ok && ld_acquire_u32(&bar[2]) == 0u;
+    }
+    __syncthreads();
+    gen += 1u;
+    return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistBufs b)
+{
+    extern __shared__ __align__(16) float sm[];
+    __shared__ double red[PT_THREADS / 32];
+    __shared__ double s_e;
+    const int TW = PT_TW, TH = b.th, V = b.V, w = b.w, h = b.h;
+    const int PW = TW + 2, QW = TW + 1;
+    const int NB = (TH + 2) * PW, NQ = (TH + 1) * QW, NP = TH * TW;
+    float *sUb = sm, *sVxb = sUb + NB, *sVyb = sVxb + NB;
+    float *sPx = sVyb + NB, *sPy = sPx + NQ, *sQx = sPy + NQ, *sQy = sQx + NQ, *sQz = sQy + NQ;
+    float *sU = sQz + NQ, *sVx = sU + NQ, *sVy = sVx + NQ;
+    float *sR = sVy + NQ, *sT11 = sR + V * NP, *sT12 = sT11 + NP, *sT22 = sT12 + NP;
+    // bar arrays: (ly, lx) in [-1, TH] x [-1, TW]; p/q: [-1, TH-1] x [-1, TW-1];
+    // u/v: [0, TH] x [0, TW]
+#define BI(ly, lx) (((ly) + 1) * PW + (lx) + 1)
+#define QI(ly, lx) (((ly) + 1) * QW + (lx) + 1)
+#define UI(ly, lx) ((ly) * QW + (lx))
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int x0 = (blockIdx.x % b.tiles_x) * TW, y0 = (blockIdx.x / b.tiles_x) * TH;
+    const size_t n = (size_t)w * h;
+    const unsigned int nblocks = gridDim.x;
+    unsigned int gen = 0;
+
+    // load the tile's state
+    for (int k = tid; k < NP; k += nthr) {
+        const int ly = k / TW, lx = k - ly * TW, x = x0 + lx, y = y0 + ly;
+        if (x >= w || y >= h) continue;
+        const size_t i = (size_t)y * w + x;
+        sU[UI(ly, lx)] = b.u[i];
+        sVx[UI(ly, lx)] = b.u1x[i];
+        sVy[UI(ly, lx)] = b.u1y[i];
+        sUb[BI(ly, lx)] = b.ubar0[i];
+        sVxb[BI(ly, lx)] = b.u1xbar0[i];
+        sVyb[BI(ly, lx)] = b.u1ybar0[i];
+        sPx[QI(ly, lx)] = b.Px[i];
+        sPy[QI(ly, lx)] = b.Py[i];
+        sQx[QI(ly, lx)] = b.Qx[i];
+        sQy[QI(ly, lx)] = b.Qy[i];
+        sQz[QI(ly, lx)] = b.Qz[i];
+        sT11[k] = b.T11[i];
+        sT12[k] = b.T12[i];
+        sT22[k] = b.T22[i];
+        for (int v = 0; v < V; ++v) sR[v * NP + k] = b.r[(size_t)v * n + i];
+    }
+    __syncthreads();
+
+    const float a1s = b.alpha1 * b.sigma, a0s = b.alpha0 * b.sigma, sl = b.sigma * b.lambda;
+    const int limit = min(b.niters, b.cap_left);
+    int k = 0, energy_at = -1, have_prev = 0, done = 0;
+    double last_e = 0.0, prev = 0.0;
+    bool ok = true;
+    while (k < limit) {
+        const int par = k & 1;
+        float *exb = b.exb[par], *exq = b.exq[par];
+        // (1) publish edges
+        for (int q = tid; q < NP; q += nthr) {
+            const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+            if (x >= w || y >= h) continue;
+            const bool right = lx == TW - 1 || x == w - 1, bottom = ly == TH - 1 || y == h - 1;
+            if (!(lx == 0 || ly == 0 || right || bottom)) continue;
+            const size_t i = (size_t)y * w + x;
+            exb[i] = sUb[BI(ly, lx)];
+            exb[n + i] = sVxb[BI(ly, lx)];
+            exb[2 * n + i] = sVyb[BI(ly, lx)];
+            if (right || bottom) {
+                exq[i] = sPx[QI(ly, lx)];
+                exq[n + i] = sPy[QI(ly, lx)];
+                exq[2 * n + i] = sQx[QI(ly, lx)];
+                exq[3 * n + i] = sQy[QI(ly, lx)];
+                exq[4 * n + i] = sQz[QI(ly, lx)];
+            }
+        }
+        // (2) barrier
+        if (!(ok = grid_barrier(b.bar, nblocks, gen))) break;
+        // (3) halo: the over-relaxations on the ring (clamped at the image
+        // border), p and q left of and above the tile
+        const int ring = 2 * (TW + 2) + 2 * TH;
+        for (int q = tid; q < ring; q += nthr) {
+            int ly, lx;
+            if (q < TW + 2) { ly = -1; lx = q - 1; }
+            else if (q < 2 * (TW + 2)) { ly = TH; lx = q - (TW + 2) - 1; }
+            else if (q < 2 * (TW + 2) + TH) { ly = q - 2 * (TW + 2); lx = -1; }
+            else { ly = q - 2 * (TW + 2) - TH; lx = TW; }
+            const int px = min(max(x0 + lx, 0), w - 1), py = min(max(y0 + ly, 0), h - 1);
+            const size_t i = (size_t)py * w + px;
+            sUb[BI(ly, lx)] = __ldcg(exb + i);
+            sVxb[BI(ly, lx)] = __ldcg(exb + n + i);
+            sVyb[BI(ly, lx)] = __ldcg(exb + 2 * n + i);
+        }
+        // tile cells beyond the image read their clamped in-image neighbour, as
+        // the fused kernel's clamped tile load does
+        for (int q = tid; q < NP; q += nthr) {
+            const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+            if (x < w && y < h) continue;
+            const int px = min(x, w - 1), py = min(y, h - 1);
+            const size_t i = (size_t)py * w + px;
+            sUb[BI(ly, lx)] = __ldcg(exb + i);
+            sVxb[BI(ly, lx)] = __ldcg(exb + n + i);
+            sVyb[BI(ly, lx)] = __ldcg(exb + 2 * n + i);
+        }
+        for (int q = tid; q < TW + TH + 1; q += nthr) {
+            const int ly = q <= TW ? -1 : q - TW - 1, lx = q <= TW ? q - 1 : -1;
+            const int px = x0 + lx, py = y0 + ly;
+            if (px < 0 || py < 0 || px >= w || py >= h) continue;
+            const size_t i = (size_t)py * w + px;
+            sPx[QI(ly, lx)] = __ldcg(exq + i);
+            sPy[QI(ly, lx)] = __ldcg(exq + n + i);
+            sQx[QI(ly, lx)] = __ldcg(exq + 2 * n + i);
+            sQy[QI(ly, lx)] = __ldcg(exq + 3 * n + i);
+            sQz[QI(ly, lx)] = __ldcg(exq + 4 * n + i);
+        }
+        __syncthreads();
+        // (4) p and q on the tile and its left / top halo (TGV2_updateP_tensor_weighed,
+        // TGV2_kernels.cu:340-365; TGV2_updateQ, :54-85), in place
+        for (int q = tid; q < (TH + 1) * (TW + 1); q += nthr) {
+            const int ly = q / (TW + 1) - 1, lx = q % (TW + 1) - 1;
+            const int px = x0 + lx, py = y0 + ly;
+            if (px < 0 || py < 0 || px >= w || py >= h) continue;
+            const int nx = px + 1 <= w - 1 ? lx + 1 : lx, ny = py + 1 <= h - 1 ? ly + 1 : ly;
+            float c11f, c12f, c22f;
+            if (lx >= 0 && ly >= 0) {
+                c11f = sT11[ly * TW + lx];
+                c12f = sT12[ly * TW + lx];
+                c22f = sT22[ly * TW + lx];
+            } else {
+                const size_t j = (size_t)py * w + px;
+                c11f = b.T11[j];
+                c12f = b.T12[j];
+                c22f = b.T22[j];
+            }
+            const int c = BI(ly, lx);
+            {
+                const double xg = sUb[BI(ly, nx)] - sUb[c] - sVxb[c];
+                const double yg = sUb[BI(ny, lx)] - sUb[c] - sVyb[c];
+                const double c11 = c11f, c12 = c12f, c22 = c22f;
+                double dx = (double)sPx[QI(ly, lx)] + (double)a1s * (c11 * xg + c12 * yg);
+                double dy = (double)sPy[QI(ly, lx)] + (double)a1s * (c12 * xg + c22 * yg);
+                proj2(dx * dx + dy * dy, dx, dy);
+                sPx[QI(ly, lx)] = (float)dx;
+                sPy[QI(ly, lx)] = (float)dy;
+            }
+            {
+                const float dx_u1x = sVxb[BI(ly, nx)] - sVxb[c];
+                const float dy_u1x = sVxb[BI(ny, lx)] - sVxb[c];
+                const float dx_u1y = sVyb[BI(ly, nx)] - sVyb[c];
+                const float dy_u1y = sVyb[BI(ny, lx)] - sVyb[c];
+                double dx = sQx[QI(ly, lx)] + a0s * dx_u1x;
+                double dy = sQy[QI(ly, lx)] + a0s * dy_u1y;
+                double dz = sQz[QI(ly, lx)] + a0s * (dy_u1x + dx_u1y) / 2.0f;
+                proj3(dx * dx + dy * dy + dz * dz + dz * dz, dx, dy, dz);
+                sQx[QI(ly, lx)] = (float)dx;
+                sQy[QI(ly, lx)] = (float)dy;
+                sQz[QI(ly, lx)] = (float)dz;
+            }
+        }
+        __syncthreads();
+        // (5) r, u, v (TGV2_updateR, TGV2_kernels.cu:87-105; TGV2_updateU_tensor_weighed, :300-338)
+        for (int q = tid; q < NP; q += nthr) {
+            const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+            if (x >= w || y >= h) continue;
+            const size_t i = (size_t)y * w + x;
+            // this pixel's L2 operands, all requested before the first use
+            float itv[PT_VMAX], iuv[PT_VMAX];
+#pragma unroll
+            for (int v = 0; v < PT_VMAX; ++v) {
+                if (v < V) {
+                    itv[v] = __ldg(b.It + (size_t)v * n + i);
+                    iuv[v] = __ldg(b.Iu + (size_t)v * n + i);
+                }
+            }
+            const float u0v = __ldg(b.u0 + i);
+            const float uold = sU[UI(ly, lx)], u1xprev = sVx[UI(ly, lx)], u1yprev = sVy[UI(ly, lx)];
+            const float du = uold - u0v;
+            float prodsum = 0.f;
+#pragma unroll
+            for (int v = 0; v < PT_VMAX; ++v) {
+                if (v < V) {
+                    const float r = proj_unit(sR[v * NP + q] + sl * (itv[v] + du * iuv[v]));
+                    sR[v * NP + q] = r;
+                    prodsum += r * iuv[v];
+                }
+            }
+            const int lxp = x > 0 ? lx - 1 : lx, lyp = y > 0 ? ly - 1 : ly;
+            const float t11 = sT11[q], t12 = sT12[q], t22 = sT22[q];
+            const float c_px = sPx[QI(ly, lx)], c_py = sPy[QI(ly, lx)];
+            const float xp_px = sPx[QI(ly, lxp)], yp_px = sPx[QI(lyp, lx)];
+            const float xp_py = sPy[QI(ly, lxp)], yp_py = sPy[QI(lyp, lx)];
+            const float unew = uold - b.tau * (-b.alpha1 * (t11 * (c_px - xp_px) + t12 * (c_py - xp_py) +
+                                                            t12 * (c_px - yp_px) + t22 * (c_py - yp_py)) +
+                                                b.lambda * prodsum);
+            const float qx = sQx[QI(ly, lx)], qy = sQy[QI(ly, lx)], qz = sQz[QI(ly, lx)];
+            const float u1xn = u1xprev - b.tau * (-b.alpha1 * (t11 * c_px + t12 * c_py) -
+                                                  b.alpha0 * (qx - sQx[QI(ly, lxp)] + qz - sQz[QI(lyp, lx)]));
+            const float u1yn = u1yprev - b.tau * (-b.alpha1 * (t12 * c_px + t22 * c_py) -
+                                                  b.alpha0 * (qz - sQz[QI(ly, lxp)] + qy - sQy[QI(lyp, lx)]));
+            sU[UI(ly, lx)] = unew;
+            sVx[UI(ly, lx)] = u1xn;
+            sVy[UI(ly, lx)] = u1yn;
+            sUb[BI(ly, lx)] = 2 * unew - uold;
+            sVxb[BI(ly, lx)] = 2 * u1xn - u1xprev;
+            sVyb[BI(ly, lx)] = 2 * u1yn - u1yprev;
+        }
+        __syncthreads();
+        ++k;
+        // (6) energy check (energy_kernel's terms; partials summed in CTA order)
+        if (b.tol > 0 && k % b.check_every == 0) {
+            for (int q = tid; q < NP; q += nthr) {
+                const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+                if (x >= w || y >= h || (lx != 0 && ly != 0)) continue;
+                const size_t i = (size_t)y * w + x;
+                b.exu[i] = sU[UI(ly, lx)];
+                b.exu[n + i] = sVx[UI(ly, lx)];
+                b.exu[2 * n + i] = sVy[UI(ly, lx)];
+            }
+            if (!(ok = grid_barrier(b.bar, nblocks, gen))) break;
+            for (int q = tid; q < TW + TH + 1; q += nthr) {
+                // right column (x0 + TW) and bottom row (y0 + TH), clamped
+                const int ly = q <= TH ? q : TH, lx = q <= TH ? TW : q - TH - 1;
+                const int px = min(x0 + lx, w - 1), py = min(y0 + ly, h - 1);
+                const size_t i = (size_t)py * w + px;
+                sU[UI(ly, lx)] = __ldcg(b.exu + i);
+                sVx[UI(ly, lx)] = __ldcg(b.exu + n + i);
+                sVy[UI(ly, lx)] = __ldcg(b.exu + 2 * n + i);
+            }
+            __syncthreads();
+            double e = 0.0;
+            for (int q = tid; q < NP; q += nthr) {
+                const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+                if (x >= w || y >= h) continue;
+                const size_t i = (size_t)y * w + x;
+                const int lxn = x + 1 <= w - 1 ? lx + 1 : lx, lyn = y + 1 <= h - 1 ? ly + 1 : ly;
+                const float uc = sU[UI(ly, lx)], ux = sU[UI(ly, lxn)], uy = sU[UI(lyn, lx)];
+                const float vxc = sVx[UI(ly, lx)], vyc = sVy[UI(ly, lx)];
+                const double gx = (double)ux - uc - vxc;
+                const double gy = (double)uy - uc - vyc;
+                const double tx = sT11[q] * gx + sT12[q] * gy, ty = sT12[q] * gx + sT22[q] * gy;
+                double ei = b.dalpha1 * sqrt(tx * tx + ty * ty);
+                const double a = (double)sVx[UI(ly, lxn)] - vxc, bb = (double)sVy[UI(lyn, lx)] - vyc;
+                const double cc = 0.5 * (((double)sVx[UI(lyn, lx)] - vxc) + ((double)sVy[UI(ly, lxn)] - vyc));
+                ei += b.dalpha0 * sqrt(a * a + bb * bb + 2 * cc * cc);
+                float itv[PT_VMAX], iuv[PT_VMAX];
+#pragma unroll
+                for (int v = 0; v < PT_VMAX; ++v) {
+                    if (v < V) {
+                        itv[v] = __ldg(b.It + (size_t)v * n + i);
+                        iuv[v] = __ldg(b.Iu + (size_t)v * n + i);
+                    }
+                }
+                const double du = (double)uc - __ldg(b.u0 + i);
+                double ed = 0.0;
+#pragma unroll
+                for (int v = 0; v < PT_VMAX; ++v)
+                    if (v < V) ed += fabs((double)itv[v] + du * iuv[v]);
+                e += ei + b.dlambda * ed;
+            }
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+            if ((tid & 31) == 0) red[tid >> 5] = e;
+            __syncthreads();
+            if (tid == 0) {
+                double t = 0.0;
+                for (int q = 0; q < PT_THREADS / 32; ++q) t += red[q];
+                b.partial[blockIdx.x] = t;
+            }
+            if (!(ok = grid_barrier(b.bar, nblocks, gen))) break;
+            if (tid == 0) {
+                double t = 0.0;
+                for (unsigned int q = 0; q < nblocks; ++q) t += __ldcg(b.partial + q);
+                s_e = t;
+            }
+            __syncthreads();
+            last_e = s_e;
+            energy_at = k;
+            if (have_prev && fabs(prev - last_e) <= b.tol * fabs(prev)) {
+                done = 1;
+                break;
+            }
+            prev = last_e;
+            have_prev = 1;
+        }
+    }
+    if (ok) {
+        // write the state back
+        for (int q = tid; q < NP; q += nthr) {
+            const int ly = q / TW, lx = q - ly * TW, x = x0 + lx, y = y0 + ly;
+            if (x >= w || y >= h) continue;
+            const size_t i = (size_t)y * w + x;
+            b.u[i] = sU[UI(ly, lx)];
+            b.u1x[i] = sVx[UI(ly, lx)];
+            b.u1y[i] = sVy[UI(ly, lx)];
+            b.Px[i] = sPx[QI(ly, lx)];
+            b.Py[i] = sPy[QI(ly, lx)];
+            b.Qx[i] = sQx[QI(ly, lx)];
+            b.Qy[i] = sQy[QI(ly, lx)];
+            b.Qz[i] = sQz[QI(ly, lx)];
+            for (int v = 0; v < V; ++v) b.r[(size_t)v * n + i] = sR[v * NP + q];
+        }
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        b.res->iters = k;
+        b.res->energy_at = energy_at;
+        b.res->done = done;
+        b.res->err = ok ? 0 : 1;
+        b.res->energy = last_e;
+    }
+#undef BI
+#undef QI
+#undef UI
+}
+
+size_t persist_smem_bytes(int th, int V)
+{
+    const int TW = PT_TW, NB = (th + 2) * (TW + 2), NQ = (th + 1) * (TW + 1), NP = th * TW;
+    return sizeof(float) * ((size_t)3 * NB + 5 * (size_t)NQ + 3 * (size_t)NQ + (size_t)V * NP + 3 * (size_t)NP);
+}
+
 struct Layout {
     float *ref01, *T11, *T12, *T22, *u0, *u1x, *u1y, *ubar[2], *u1xbar[2], *u1ybar[2], *Px[2], *Py[2], *Qx[2],
         *Qy[2], *Qz[2], *It, *Iu, *r;
     double *partial, *energy;
+    float *exb[2], *exq[2], *exu;
+    double *ppartial;
+    unsigned int *bar;
+    PersistResult *res;
     size_t bytes;
 };
 
@@ -474,8 +915,31 @@ Layout layout(void *base, int w, int h, int V)
     L.r = take(n * V);
     L.partial = (double *)take(2 * kEnergyBlocks);
     L.energy = (double *)take(2);
+    for (int k = 0; k < 2; ++k) {
+        L.exb[k] = take(3 * n);
+        L.exq[k] = take(5 * n);
+    }
+    L.exu = take(3 * n);
+    L.ppartial = (double *)take(2 * 1024);
+    L.bar = (unsigned int *)take(64);
+    L.res = (PersistResult *)take(16);
     L.bytes = off;
     return L;
+}
+
+// Tile height for the persistent kernel, or 0 when the image does not fit on
+// chip (one 64-column tile per SM) or has more views than it keeps.
+int persist_tile_height(int w, int h, int V, int sms, size_t smem_limit)
+{
+    if (V > PT_VMAX) return 0;
+    const int tx = ceil_div(w, PT_TW);
+    if (tx > sms) return 0;
+    const int rows = sms / tx;
+    // as few rows per tile as the SM count allows, but not below 16 (small
+    // images then use fewer CTAs than SMs)
+    const int th = max(ceil_div(h, rows), min(h, 16));
+    if (th < 2 || persist_smem_bytes(th, V) > smem_limit) return 0;
+    return th;
 }
 
 }  // namespace
@@ -536,6 +1000,35 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     ib.tau = prm->tau;
     ib.sigma = prm->sigma;
     const dim3 gi(ceil_div(w, TX), ceil_div(h, TY)), bi(TX, TY);
+
+    // on-chip persistent iterations when the image fits one tile per SM
+    int pth = 0, ptiles = 0;
+    size_t psmem = 0;
+    if (prm->iteration_kernel == MVS_TGV2_ITER_AUTO) {
+        int dev = 0, sms = 0, coop = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        const size_t limit = optin > 4096 ? (size_t)optin - 4096 : 0;   // room for the static shared memory
+        pth = coop ? persist_tile_height(w, h, V, sms, limit) : 0;
+        // one iteration of the persistent kernel is a chain of dependent grid
+        // round trips (barrier, halo, L2 operands) that a partly filled GPU
+        // cannot hide: below 3/4 of the SMs one launch per iteration is faster
+        if (pth && ceil_div(w, PT_TW) * ceil_div(h, pth) * 4 < sms * 3) pth = 0;
+        if (pth) {
+            psmem = persist_smem_bytes(pth, V);
+            ptiles = ceil_div(w, PT_TW) * ceil_div(h, pth);
+            int per_sm = 0;
+            if (cudaFuncSetAttribute(tgv2_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)psmem) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tgv2_persistent_kernel, PT_THREADS, psmem) !=
+                    cudaSuccess ||
+                per_sm * sms < ptiles)
+                pth = 0;
+            cudaGetLastError();   // a refused attribute or query is not an error of this call
+        }
+    }
     for (int l = 0; l < prm->warps && !done; ++l) {
         if (warm && l == 0)
             warm_init_kernel<<<eg, 256, 0, st>>>(n, V, warm->u_lin, u, warm->v, warm->v ? warm->v + n : nullptr, L.u0,
@@ -556,6 +1049,75 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         rc = check_launch("tgv2 linearisation");
         if (rc) break;
         cur = 0;
+        if (pth) {
+            // the whole linearisation in one cooperative launch
+            PersistBufs pb;
+            pb.T11 = L.T11;
+            pb.T12 = L.T12;
+            pb.T22 = L.T22;
+            pb.u0 = L.u0;
+            pb.It = L.It;
+            pb.Iu = L.Iu;
+            pb.u = u;
+            pb.u1x = L.u1x;
+            pb.u1y = L.u1y;
+            pb.r = L.r;
+            pb.ubar0 = L.ubar[0];
+            pb.u1xbar0 = L.u1xbar[0];
+            pb.u1ybar0 = L.u1ybar[0];
+            pb.Px = L.Px[0];
+            pb.Py = L.Py[0];
+            pb.Qx = L.Qx[0];
+            pb.Qy = L.Qy[0];
+            pb.Qz = L.Qz[0];
+            for (int q = 0; q < 2; ++q) {
+                pb.exb[q] = L.exb[q];
+                pb.exq[q] = L.exq[q];
+            }
+            pb.exu = L.exu;
+            pb.partial = L.ppartial;
+            pb.bar = L.bar;
+            pb.res = L.res;
+            pb.w = w;
+            pb.h = h;
+            pb.V = V;
+            pb.tiles_x = ceil_div(w, PT_TW);
+            pb.th = pth;
+            pb.niters = prm->niters;
+            pb.cap_left = cap - total;
+            pb.check_every = check_every;
+            pb.tol = prm->tol;
+            pb.lambda = prm->lambda;
+            pb.alpha0 = prm->alpha0;
+            pb.alpha1 = prm->alpha1;
+            pb.tau = prm->tau;
+            pb.sigma = prm->sigma;
+            pb.dlambda = prm->lambda;
+            pb.dalpha0 = prm->alpha0;
+            pb.dalpha1 = prm->alpha1;
+            cudaMemsetAsync(L.bar, 0, 64, st);
+            void *args[] = {&pb};
+            cudaError_t e = cudaLaunchCooperativeKernel((const void *)tgv2_persistent_kernel, dim3(ptiles),
+                                                        dim3(PT_THREADS), args, psmem, st);
+            PersistResult hr{};
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&hr, L.res, sizeof(hr), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                rc = set_error(MVS_ERR_CUDA, "tgv2 persistent iteration: %s", cudaGetErrorString(e));
+                break;
+            }
+            if (hr.err) {
+                rc = set_error(MVS_ERR_TIMEOUT, "tgv2 persistent iteration: a grid barrier wait gave up");
+                break;
+            }
+            if (hr.energy_at >= 0) {
+                last_e = hr.energy;
+                energy_at = total + hr.energy_at;
+            }
+            total += hr.iters;
+            done = hr.done || total >= cap;
+            continue;
+        }
         bool have_prev = false;
         double prev = 0.0;
         for (int k = 0; k < prm->niters; ++k) {

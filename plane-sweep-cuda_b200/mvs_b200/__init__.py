@@ -62,7 +62,8 @@ class SweepDesc(C.Structure):
 class TGV2Params(C.Structure):
     _fields_ = [("niters", C.c_int32), ("warps", C.c_int32), ("lam", C.c_double), ("alpha0", C.c_double),
                 ("alpha1", C.c_double), ("tau", C.c_double), ("sigma", C.c_double), ("beta", C.c_double),
-                ("gamma", C.c_double), ("tol", C.c_double), ("check_every", C.c_int32), ("max_iters", C.c_int32)]
+                ("gamma", C.c_double), ("tol", C.c_double), ("check_every", C.c_int32), ("max_iters", C.c_int32),
+                ("iteration_kernel", C.c_int32)]
 
 
 class TVL1Params(C.Structure):
@@ -263,9 +264,13 @@ def sweep_wta_volume(cost, depths, n_pixels, n_planes, zfar, depth_out, labels=N
 # TGV2 / TV-L1 (device tensors)
 # ---------------------------------------------------------------------------
 
+TGV2_ITER_AUTO, TGV2_ITER_LAUNCH = 0, 1
+
+
 def tgv2_params(niters=30, warps=15, lam=0.5, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0,
-                tol=0.0, check_every=10, max_iters=0):
-    return TGV2Params(niters, warps, lam, alpha0, alpha1, tau, sigma, beta, gamma, tol, check_every, max_iters)
+                tol=0.0, check_every=10, max_iters=0, iteration_kernel=TGV2_ITER_AUTO):
+    return TGV2Params(niters, warps, lam, alpha0, alpha1, tau, sigma, beta, gamma, tol, check_every, max_iters,
+                      iteration_kernel)
 
 
 def float_cams(K_1based, rel_poses):
