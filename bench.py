@@ -182,6 +182,78 @@ def run_reference(args):
     return 0
 
 
+def run_reference_gpu(fr, planes, dev, d_ref, d_srcs, wta_depth):
+    """The reference's RunAlgorithm and TGV call sequences with its own kernels compiled for
+    this GPU (oracle/_ref/libmvs_ref_gpu.so), beside this engine in the reference's arithmetic
+    (per-view sweep, reference moments, the reference's float homographies) on the same frame."""
+    import torch
+    import mvs_b200 as M
+    from mvs_b200 import hostmath as hm
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+    if po.ref_gpu_lib() is None:
+        return {"unavailable": "oracle/_ref/libmvs_ref_gpu.so was not built (needs the reference tree)"}
+    K1 = np.float32(fr.ref_cam.K_1based)
+    poses = [(np.float32(c.R), np.float32(c.t)) for c in fr.src_cams]
+    Rref, tref = np.float32(fr.ref_cam.R), np.float32(fr.ref_cam.t)
+    evals = W * H * P * V
+    out = {"kernels": "the reference's kernels.cu / TGV2_kernels.cu, unchanged, nvcc sm_100a",
+           "sweep": {}, "tgv2_500_iterations": {}}
+    ms = []
+    for k in range(2):
+        _, t = po.ref_gpu_sweep(fr.ref, fr.srcs, K1, Rref, tref, poses, planes, WIN, 8.0)
+        if t < 0:
+            return {"unavailable": "a CUDA error in the reference's kernels"}
+        if k:
+            ms.append(t)
+    out["sweep"]["reference_ms"] = min(ms)
+    out["sweep"]["reference_value"] = evals / (min(ms) / 1e3) / 1e6
+    # this engine, reference arithmetic: per-view sweep + combine, reference float homographies
+    iK = hm.inv3_f32(K1)
+    rel = [hm.relative_f32(fr.ref_cam.R, fr.ref_cam.t, c.R, c.t) for c in fr.src_cams]
+    Hh = np.stack([np.stack([hm.homography_f32(K1, iK, r[0], r[1], np.float32(d)).reshape(9) for d in planes])
+                   for r in rel]).astype(np.float32)
+    d_H = torch.from_numpy(Hh.reshape(-1)).to(dev)
+    d_planes = torch.from_numpy(planes).to(dev)
+    desc = M.sweep_desc(W, H, V, P, WIN, M.MOMENTS_REFERENCE, M.SWEEP_PER_VIEW, 1e-4, 0.5, 8.0)
+    depth = torch.empty((H, W), device=dev)
+    ws = torch.empty(M.sweep_workspace_bytes(desc) // 8 + 1, dtype=torch.int64, device=dev)
+    em = []
+    for k in range(4):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        M.sweep(desc, d_ref, d_srcs, d_H, d_planes, depth, None, None, None, ws)
+        b.record()
+        torch.cuda.synchronize()
+        if k:
+            em.append(a.elapsed_time(b))
+    out["sweep"]["this_engine_reference_arithmetic_ms"] = min(em)
+    out["sweep"]["this_engine_reference_arithmetic_value"] = evals / (min(em) / 1e3) / 1e6
+    out["sweep"]["speedup"] = min(ms) / min(em)
+    if wta_depth is not None:
+        u0 = wta_depth.cpu().numpy()
+        _, t = po.ref_gpu_tgv(fr.ref, fr.srcs, K1, Rref, tref, poses, 500, 1, u_init=u0)
+        out["tgv2_500_iterations"]["reference_ms"] = t
+        Kf, Rs = K1.reshape(9), np.stack([r[0].reshape(9) for r in rel])
+        ts = np.stack([r[1] for r in rel])
+        prm = M.tgv2_params(niters=500, warps=1)
+        u = torch.empty((H, W), device=dev)
+        tw = torch.empty(M.tgv2_workspace_bytes(W, H, V) // 8 + 1, dtype=torch.int64, device=dev)
+        tm = []
+        for k in range(3):
+            u.copy_(wta_depth)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            M.tgv2_run(d_ref, d_srcs, Kf, iK.reshape(9), Rs, ts, prm, u, u_from_input=True, workspace=tw)
+            b.record()
+            torch.cuda.synchronize()
+            if k:
+                tm.append(a.elapsed_time(b))
+        out["tgv2_500_iterations"]["this_engine_ms"] = min(tm)
+        out["tgv2_500_iterations"]["speedup"] = t / min(tm)
+    return out
+
+
 def run_batched(args, dev, stream, flush, rank):
     """the mixed 48-frame batch through mvs_batch (one graph launch per batch)."""
     import time
@@ -273,6 +345,8 @@ def main():
                     help="skip the learned TGV2 warm start")
     ap.add_argument("--warm-frames", type=int, default=8)
     ap.add_argument("--no-batch", dest="batch", action="store_false", help="skip the batched-frames workload")
+    ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
+                    help="skip timing the reference's own CUDA kernels on this GPU")
     ap.add_argument("--batch-frames", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fusion", dest="fusion", action="store_false")
@@ -414,6 +488,12 @@ def main():
                 "dual_start": {"sigma_pq": WS.WARM_DUAL_SIGMA, "sigma_r": WS.WARM_DUAL_SIGMA_R},
                 "network": {"weights": WS.WEIGHTS.name, "trained": wmeta},
                 "includes": "network forward + TGV2 to tolerance; scenes rendered on the device, seeds held out"}
+
+    # --- the reference's own CUDA kernels on this GPU, same frame and plane list (context for the
+    #     ratios: the same evaluations, one launch per reference wrapper call) ---
+    ref_gpu = None
+    if args.reference_gpu and rank == 0:
+        ref_gpu = run_reference_gpu(fr, planes, dev, d_ref, d_srcs, wta_depth if tgv_ms else None)
 
     # --- batched uneven frames: 48 frames (320x240 / 640x480 rooms, 1242x375 street)
     #     with 64-256 planes, 4-8 views and 5x5-11x11 windows in one graph launch; the autotuner
@@ -568,6 +648,7 @@ def main():
                 "d2h_bytes_per_step": W * H * 4, "api": "mvs_ps_* PlaneSweep handle (RunAlgorithm + getDepthmap)"},
         "fusion": fusion,
         "batched": batched,
+        "reference_gpu": ref_gpu,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clock_summary,
     }

@@ -213,6 +213,68 @@ def ref_sweep(ref, srcs, K_1based, Rref, tref, src_poses, planes, winsize, znear
     return dict(depth=out, best=best, vdepth=vdepth, seconds=secs)
 
 
+_ref_gpu = None
+
+
+def ref_gpu_lib():
+    """The reference's own CUDA kernels compiled for the B200, or None if not built."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        path = HERE / "_ref" / "libmvs_ref_gpu.so"
+        if not path.exists():
+            return None
+        L = C.CDLL(str(path))
+        P = _F
+        L.ref_gpu_sweep.restype = C.c_double
+        L.ref_gpu_sweep.argtypes = [C.c_int, C.c_int, P, P, C.c_int, P, P, P, P, P, C.c_int, P, C.c_int,
+                                    C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, P]
+        L.ref_gpu_tgv.restype = C.c_double
+        L.ref_gpu_tgv.argtypes = ([C.c_int, C.c_int, P, P, C.c_int, P, P, P, P, P, C.c_int, C.c_int, C.c_int] +
+                                  [C.c_double] * 7 + [P, P])
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def ref_gpu_sweep(ref, srcs, K_1based, Rref, tref, src_poses, planes, winsize, zfar, stdthresh=1e-4,
+                  nccthresh=0.5, alternative=False):
+    """The reference's RunAlgorithm call sequence with its own kernels on the
+    GPU; returns (depth, device ms of the compute)."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref/libmvs_ref_gpu.so not built")
+    h, w = ref.shape
+    V = len(srcs)
+    S = _f32(np.stack(srcs))
+    Rs = _f32(np.stack([p[0] for p in src_poses]))
+    ts = _f32(np.stack([p[1] for p in src_poses]))
+    out = np.zeros((h, w), np.float32)
+    pl = _f32(planes)
+    ms = L.ref_gpu_sweep(w, h, _fp(_f32(ref)), _fp(S), V, _fp(_f32(K_1based)), _fp(_f32(Rref)), _fp(_f32(tref)),
+                         _fp(Rs), _fp(ts), int(alternative), _fp(pl), len(pl), float(pl[0]), float(zfar), winsize,
+                         stdthresh, nccthresh, _fp(out))
+    return out, ms
+
+
+def ref_gpu_tgv(ref, srcs, K_1based, Rref, tref, src_poses, niters, warps, u_init=None, lam=0.5, alpha0=2.0,
+                alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0, alternative=False):
+    """The reference's PlaneSweep::TGV call sequence with its own kernels on the
+    GPU; returns (u, device ms of the iterations)."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref/libmvs_ref_gpu.so not built")
+    h, w = ref.shape
+    V = len(srcs)
+    S = _f32(np.stack(srcs))
+    Rs = _f32(np.stack([p[0] for p in src_poses]))
+    ts = _f32(np.stack([p[1] for p in src_poses]))
+    out = np.zeros((h, w), np.float32)
+    ui = None if u_init is None else _f32(u_init)
+    ms = L.ref_gpu_tgv(w, h, _fp(_f32(ref)), _fp(S), V, _fp(_f32(K_1based)), _fp(_f32(Rref)), _fp(_f32(tref)),
+                       _fp(Rs), _fp(ts), int(alternative), niters, warps, lam, alpha0, alpha1, tau, sigma, beta,
+                       gamma, _fp(ui), _fp(out))
+    return out, ms
+
+
 def labels_from_depth(vdepth, planes):
     """Per-view plane index from the reference's stored depth (0 -> -1)."""
     planes = np.asarray(planes, np.float32)

@@ -79,7 +79,7 @@ def build_oracle(verbose: bool = False) -> None:
     """The C oracle always; the reference compiled for the CPU when its tree is present."""
     targets = ["oracle"]
     if (REFERENCE_SRC / "kernels.cu").exists():
-        targets.append("ref")
+        targets += ["ref", "ref_gpu"]
     r = subprocess.run(["make", "-C", str(ORACLE), *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
