@@ -568,12 +568,15 @@ def main():
     ps.setNumberofImages(V)
     ps.setZ(0.4, 8.0)
     ps.setSweepOptions(M.MOMENTS_COMPENSATED, M.SWEEP_AGGREGATED, True)
-    Rsrc = [c.R for c in fr.src_cams]
-    tsrc = [c.t for c in fr.src_cams]
+    Rsrc = np.stack([c.R for c in fr.src_cams]).astype(np.float32)
+    tsrc = np.stack([c.t for c in fr.src_cams]).astype(np.float32)
+    # the caller's host images: the reference and one (V, H, W) array of sources
+    h_ref = np.ascontiguousarray(fr.ref, dtype=np.float32)
+    h_srcs = np.ascontiguousarray(np.stack(fr.srcs), dtype=np.float32)
 
     def e2e_step():
-        ps.set_reference(fr.ref, fr.ref_cam.R, fr.ref_cam.t)
-        ps.set_sources(fr.srcs, Rsrc, tsrc)
+        ps.set_reference(h_ref, fr.ref_cam.R, fr.ref_cam.t)
+        ps.set_sources(h_srcs, Rsrc, tsrc)
         ps.RunAlgorithm()
         return ps.getDepthmap()
 

@@ -40,6 +40,10 @@ extern "C" {
 const char *mvs_last_error(void);
 /* 10000 * major + 100 * minor + patch. */
 int mvs_version(void);
+/* Page-locked host memory (falls back to ordinary memory if page-locking
+ * fails); free it with mvs_host_free.  The C++ layer keeps host images in it. */
+void *mvs_host_alloc(size_t bytes);
+void mvs_host_free(void *p);
 /* Select the device for the calling thread (replaces PlaneSweep::cudaDevInit,
  * planesweep.cpp:30-58, without the device reset of cudaReset()). */
 int mvs_set_device(int device);

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <new>
 #include <vector>
 
 #include "mvs_b200.h"
@@ -134,7 +135,31 @@ inline Vector3D operator-(const Vector3D &a, const Vector3D &b) { return Vector3
 
 /* ---- images ------------------------------------------------------------------ */
 
-/* Host image, dense (pitch == width * sizeof(T)), with its world->camera pose. */
+/* Allocator of page-locked host memory (mvs_host_alloc): host images that the
+ * library uploads or downloads then move at full PCIe / C2C speed. */
+template <typename T>
+struct PinnedAllocator {
+    typedef T value_type;
+    PinnedAllocator() {}
+    template <typename U>
+    PinnedAllocator(const PinnedAllocator<U> &) {}
+    T *allocate(size_t n)
+    {
+        void *p = mvs_host_alloc(n * sizeof(T));
+        if (!p) throw std::bad_alloc();
+        return static_cast<T *>(p);
+    }
+    void deallocate(T *p, size_t) { mvs_host_free(p); }
+    template <typename U>
+    bool operator==(const PinnedAllocator<U> &) const { return true; }
+    template <typename U>
+    bool operator!=(const PinnedAllocator<U> &) const { return false; }
+};
+
+/* Host image, dense (pitch == width * sizeof(T)), with its world->camera pose.
+ * reset() keeps the storage when the size does not change (the contents are
+ * then the previous image's, as the reference's re-allocated images hold
+ * whatever the allocator returns). */
 template <typename T>
 class CamImage {
 public:
@@ -142,7 +167,7 @@ public:
     Vector3D t;
     CamImage() : w_(0), h_(0) {}
     CamImage(size_t w, size_t h) : w_(w), h_(h), px_(w * h) {}
-    void reset(size_t w, size_t h) { w_ = w; h_ = h; px_.assign(w * h, T()); }
+    void reset(size_t w, size_t h) { w_ = w; h_ = h; px_.resize(w * h); }
     T *data() { return px_.data(); }
     const T *data() const { return px_.data(); }
     size_t width() const { return w_; }
@@ -153,7 +178,7 @@ public:
 
 private:
     size_t w_, h_;
-    std::vector<T> px_;
+    std::vector<T, PinnedAllocator<T>> px_;
 };
 
 /* ---- PlaneSweep ----------------------------------------------------------------- */

@@ -119,6 +119,35 @@ const char *mvs_last_error(void) { return g_err; }
 
 int mvs_version(void) { return 1 * 10000 + 0 * 100 + 0; }
 
+// Page-locked allocations are tagged with a header so that a fall-back
+// malloc (when page-locking fails) is freed the right way.
+struct HostBlock {
+    int pinned;
+    int pad[3];
+};
+
+void *mvs_host_alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes + sizeof(HostBlock)) == cudaSuccess && p) {
+        ((HostBlock *)p)->pinned = 1;
+        return (char *)p + sizeof(HostBlock);
+    }
+    cudaGetLastError();
+    p = malloc(bytes + sizeof(HostBlock));
+    if (!p) return nullptr;
+    ((HostBlock *)p)->pinned = 0;
+    return (char *)p + sizeof(HostBlock);
+}
+
+void mvs_host_free(void *q)
+{
+    if (!q) return;
+    HostBlock *b = (HostBlock *)((char *)q - sizeof(HostBlock));
+    if (b->pinned) cudaFreeHost(b);
+    else free(b);
+}
+
 int mvs_set_device(int device)
 {
     clear_error();
@@ -152,7 +181,7 @@ static int check_sweep_desc(const mvs_sweep_desc *d)
 size_t mvs_sweep_workspace_bytes(const mvs_sweep_desc *d)
 {
     if (check_sweep_desc(d)) return 0;
-    // winner words, then (aggregated mode) the sources' 2x2 neighbourhoods
+    // winner words, then the sources' 2x2 neighbourhoods
     return (sweep_scratch_bytes(d) + 255) / 256 * 256 + sweep_quad_bytes(d);
 }
 
@@ -187,7 +216,7 @@ int mvs_sweep(const mvs_sweep_desc *d, const float *ref, const float *srcs, cons
     if (((uintptr_t)ws) & 7) return set_error(MVS_ERR_ARG, "workspace must be 8-byte aligned");
     if (d->mode == MVS_SWEEP_PER_VIEW && cost) return set_error(MVS_ERR_ARG, "cost volume is an aggregated-mode output");
     const int chunks = sweep_pick_chunks(d->window, d->width, d->height, d->n_views, d->n_planes, d->mode);
-    float4 *quad = sweep_quad_bytes(d) ? (float4 *)((char *)ws + (sweep_scratch_bytes(d) + 255) / 256 * 256) : nullptr;
+    float4 *quad = (float4 *)((char *)ws + (sweep_scratch_bytes(d) + 255) / 256 * 256);
     return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)ws, chunks, stream,
                         quad);
 }

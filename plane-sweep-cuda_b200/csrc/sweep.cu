@@ -393,86 +393,6 @@ __device__ __forceinline__ float tile_shift(Smem &S)
     return t / (float)(G::RH * G::RW);
 }
 
-// ---- per-view kernel -------------------------------------------------------------
-// grid: (tiles_x, tiles_y, V * n_chunks)
-
-template <int WIN, int MOM>
-__global__ void __launch_bounds__(THREADS, 2) sweep_view_kernel(SweepArgs a)
-{
-    using G = Geo<WIN>;
-    __shared__ Smem S;
-    const int view = blockIdx.z / a.n_chunks, chunk = blockIdx.z % a.n_chunks;
-    const int x0 = blockIdx.x * G::TW, y0 = blockIdx.y * TH;
-    const int w = a.w, h = a.h;
-    const float *src = a.srcs + (size_t)view * w * h;
-
-    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
-    __syncthreads();
-    const float shift = tile_shift<WIN, MOM>(S);
-    float refcol[G::SROWS];
-    {
-        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
-#pragma unroll
-        for (int i = 0; i < G::SROWS; ++i) {
-            const float r = (c < G::RW) ? S.Wt[8 * s + i][c] : 0.f;
-            refcol[i] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
-        }
-    }
-    float rm[G::RUN], rs[G::RUN];
-    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
-    float Xcol, Ycol[A0Cells<WIN>::CELLS];
-    a0_setup<WIN>(w, h, x0, y0, Xcol, Ycol);
-
-    float best[G::RUN];
-    int lab[G::RUN];
-#pragma unroll
-    for (int j = 0; j < G::RUN; ++j) {
-        best[j] = 0.f;
-        lab[j] = -1;
-    }
-    const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
-    const float *Hv = a.H + (size_t)view * a.P * 9;
-    for (int p = p0; p < p1; ++p) {
-        if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(Hv + (size_t)p * 9 + threadIdx.x);
-        __syncthreads();   // Hm visible; previous plane's pass B finished with CS
-        float Hm[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-        pass_a0<WIN, MOM>(S.Wt, src, w, h, Hm, Xcol, Ycol);
-        __syncthreads();
-        pass_a1<WIN, MOM>(S.Wt, S.CS, refcol, shift);
-        __syncthreads();
-        float s1[G::RUN], s2[G::RUN], s12[G::RUN];
-        row_sums<WIN, MOM>(S.CS, 0, s1);
-        row_sums<WIN, MOM>(S.CS, 1, s2);
-        row_sums<WIN, MOM>(S.CS, 2, s12);
-#pragma unroll
-        for (int j = 0; j < G::RUN; ++j) {
-            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
-            if (c > best[j]) {
-                best[j] = c;
-                lab[j] = p;
-            }
-        }
-    }
-    // results: (ncc bits << 32) | ~plane, so that a 64-bit max keeps the
-    // largest NCC and, among equal NCCs, the earliest plane.
-    const int y = y0 + (threadIdx.x >> 3);
-    if (y >= h) return;
-    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
-    unsigned long long *outp = a.packed + (size_t)view * w * h + (size_t)y * w;
-#pragma unroll
-    for (int j = 0; j < G::RUN; ++j) {
-        const int x = xb + j;
-        if (x >= w) break;
-        unsigned long long key = 0ull;
-        if (lab[j] >= 0)
-            key = ((unsigned long long)__float_as_uint(best[j]) << 32) | (unsigned long long)(0xffffffffu - (unsigned)lab[j]);
-        if (a.n_chunks == 1) outp[x] = key;
-        else if (key) atomicMax(outp + x, key);
-    }
-}
-
 // ---- aggregated mode: cost = 1 - mean NCC over views, BF16 WTA -------------------
 //
 // The per-CTA state that the per-view kernel keeps in registers -- the
@@ -749,6 +669,97 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
         unsigned long long *o = a.wta + (size_t)y * w + x;
         if (a.n_chunks == 1) *o = key;
         else if (any) atomicMin(o, key);
+    }
+}
+
+// ---- per-view kernel -------------------------------------------------------------
+// grid: (tiles_x, tiles_y, V * n_chunks); dynamic shared memory: sizeof(AggSmem).
+// The per-CTA reference state sits in shared memory as in the aggregated
+// kernel, so it also runs three CTAs per SM.
+
+template <int WIN, int MOM>
+__global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
+{
+    using G = Geo<WIN>;
+    extern __shared__ __align__(16) unsigned char view_smem[];
+    AggSmem &A = *reinterpret_cast<AggSmem *>(view_smem);
+    Smem &S = A.S;
+    const int view = blockIdx.z / a.n_chunks, chunk = blockIdx.z % a.n_chunks;
+    const int x0 = blockIdx.x * G::TW, y0 = blockIdx.y * TH;
+    const int w = a.w, h = a.h;
+    const size_t n = (size_t)w * h;
+    const float *src = a.srcs + (size_t)view * n;
+    const float4 *quad = a.quad ? a.quad + (size_t)view * n : nullptr;
+
+    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    for (int i = threadIdx.x; i < G::RH; i += THREADS) A.Yc[i] = (float)(mirror_idx(y0 - G::R + i, h) + 1);
+    __syncthreads();
+    const float shift = tile_shift<WIN, MOM>(S);
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
+        A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+    }
+    {
+        float rm[G::RUN], rs[G::RUN];
+        ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
+        const int yy = threadIdx.x >> 3, g = threadIdx.x & 7;
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) {
+            A.RM[yy][g * G::RUN + j] = rm[j];
+            A.RS[yy][g * G::RUN + j] = rs[j];
+        }
+    }
+    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x & 63), w) + 1);
+    const int ly = threadIdx.x >> 3, lx = (threadIdx.x & 7) * G::RUN;
+
+    float best[G::RUN];
+    int lab[G::RUN];
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        best[j] = 0.f;
+        lab[j] = -1;
+    }
+    const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
+    const float *Hv = a.H + (size_t)view * a.P * 9;
+    for (int p = p0; p < p1; ++p) {
+        if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(Hv + (size_t)p * 9 + threadIdx.x);
+        __syncthreads();   // Hm visible; previous plane's pass B finished with CS
+        float Hm[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
+        pass_a0_rows<WIN, MOM>(S.Wt, src, quad, w, h, Hm, Xcol, A.Yc);
+        __syncthreads();
+        pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf, shift);
+        __syncthreads();
+        float s1[G::RUN], s2[G::RUN], s12[G::RUN];
+        row_sums<WIN, MOM>(S.CS, 0, s1);
+        row_sums<WIN, MOM>(S.CS, 1, s2);
+        row_sums<WIN, MOM>(S.CS, 2, s12);
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) {
+            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], A.RM[ly][lx + j], A.RS[ly][lx + j], a.stdthresh);
+            if (c > best[j]) {
+                best[j] = c;
+                lab[j] = p;
+            }
+        }
+    }
+    // results: (ncc bits << 32) | ~plane, so that a 64-bit max keeps the
+    // largest NCC and, among equal NCCs, the earliest plane.
+    const int y = y0 + (threadIdx.x >> 3);
+    if (y >= h) return;
+    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
+    unsigned long long *outp = a.packed + (size_t)view * w * h + (size_t)y * w;
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        const int x = xb + j;
+        if (x >= w) break;
+        unsigned long long key = 0ull;
+        if (lab[j] >= 0)
+            key = ((unsigned long long)__float_as_uint(best[j]) << 32) | (unsigned long long)(0xffffffffu - (unsigned)lab[j]);
+        if (a.n_chunks == 1) outp[x] = key;
+        else if (key) atomicMax(outp + x, key);
     }
 }
 
@@ -1035,8 +1046,12 @@ int launch_window(int win, const SweepArgs &a, int mode, void *stream)
     case WIN: {                                                                                      \
         dim3 grid(ceil_div(a.w, Geo<WIN>::TW), ceil_div(a.h, TH),                                    \
                   mode == MVS_SWEEP_PER_VIEW ? a.V * a.n_chunks : a.n_chunks);                       \
-        if (mode == MVS_SWEEP_PER_VIEW) sweep_view_kernel<WIN, MOM><<<grid, THREADS, 0, st>>>(a);   \
-        else {                                                                                       \
+        if (mode == MVS_SWEEP_PER_VIEW) {                                                            \
+            MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_view_kernel<WIN, MOM>,                              \
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+                                              (int)sizeof(AggSmem)));                                    \
+            sweep_view_kernel<WIN, MOM><<<grid, THREADS, sizeof(AggSmem), st>>>(a);                    \
+        } else {                                                                                     \
             MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_aggregated_kernel<WIN, MOM>,                        \
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,              \
                                               (int)sizeof(AggSmem)));                                    \
@@ -1084,7 +1099,7 @@ size_t sweep_scratch_bytes(const mvs_sweep_desc *d)
 
 size_t sweep_quad_bytes(const mvs_sweep_desc *d)
 {
-    return d->mode == MVS_SWEEP_AGGREGATED ? (size_t)d->width * d->height * d->n_views * sizeof(float4) : 0;
+    return (size_t)d->width * d->height * d->n_views * sizeof(float4);
 }
 
 int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, const float *H, const float *depths,
@@ -1110,7 +1125,7 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     a.wta = nullptr;
     a.cost = nullptr;
     a.quad = nullptr;
-    if (d->mode == MVS_SWEEP_AGGREGATED && quad) {
+    if (quad) {
         const size_t total = (size_t)n * d->n_views;
         const size_t blocks = (total + 255) / 256 < (size_t)16 * kSMs ? (total + 255) / 256 : (size_t)16 * kSMs;
         quad_kernel<<<(int)blocks, 256, 0, st>>>(srcs, d->n_views, d->width, d->height, quad);

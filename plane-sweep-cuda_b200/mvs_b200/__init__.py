@@ -100,6 +100,8 @@ def _sig(name, res, *args):
 _sig("mvs_last_error", C.c_char_p)
 _sig("mvs_version", C.c_int)
 _sig("mvs_set_device", C.c_int, C.c_int)
+_sig("mvs_host_alloc", C.c_void_p, C.c_size_t)
+_sig("mvs_host_free", None, C.c_void_p)
 _sig("mvs_sweep_workspace_bytes", C.c_size_t, C.POINTER(SweepDesc))
 _sig("mvs_sweep_homographies", C.c_int, C.POINTER(SweepDesc), _D, _D, _D, _VP, _VP, _VP)
 _sig("mvs_sweep", C.c_int, C.POINTER(SweepDesc), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_size_t, _VP)
@@ -633,7 +635,9 @@ class PlaneSweep:
     def set_sources(self, imgs, Rs, ts):
         imgs = _f32(np.stack(imgs)) if isinstance(imgs, (list, tuple)) else _f32(imgs)
         self.n_views = imgs.shape[0]
-        check(_L.mvs_ps_set_sources(self.h, _fp(imgs), imgs.shape[0], _fp(_f32(np.stack(Rs))), _fp(_f32(np.stack(ts)))))
+        Rs = _f32(Rs if isinstance(Rs, np.ndarray) else np.stack(Rs))
+        ts = _f32(ts if isinstance(ts, np.ndarray) else np.stack(ts))
+        check(_L.mvs_ps_set_sources(self.h, _fp(imgs), imgs.shape[0], _fp(Rs), _fp(ts)))
 
     def setK(self, K):
         check(_L.mvs_ps_set_K(self.h, _fp(_f32(K))))

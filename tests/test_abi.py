@@ -42,7 +42,8 @@ def test_sweep_descriptor_validation(field, value):
 
 def test_sweep_workspace_sizes():
     d = M.sweep_desc(640, 480, 8, 256, 9)
-    assert M.sweep_workspace_bytes(d) == 640 * 480 * 8 * 8
+    # per view: one winner word per pixel and view, then each source pixel's 2x2 neighbourhood
+    assert M.sweep_workspace_bytes(d) == 640 * 480 * 8 * 8 + 640 * 480 * 8 * 16
     d.mode = M.SWEEP_AGGREGATED
     # one winner word per pixel, then each source pixel's 2x2 neighbourhood (16 bytes per view)
     assert M.sweep_workspace_bytes(d) == 640 * 480 * 8 + 640 * 480 * 8 * 16
