@@ -308,6 +308,22 @@ int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out);
 int mvs_ps_get_view_best(mvs_planesweep *ps, float *out);
 int mvs_ps_get_3d_coordinates(mvs_planesweep *ps, float *X, float *Y, float *Z); /* get3Dcoordinates */
 int mvs_ps_get_plane_count(mvs_planesweep *ps, int32_t *n);
+/* ---- data formats either side of the path ---------------------------------
+ * ICL-NUIM camera file (Reader::getcamParameters / getcamK / computeRT,
+ * reader.cpp:181-296): the cam_pos, cam_dir, cam_up and cam_right lines give
+ * the 1-based K of a width x height image (negative fy), the camera->world
+ * rotation R (columns: right, down, forward) and t = cam_pos, in the reader's
+ * float arithmetic; the pose is for PlaneSweep's alternative relative-matrix
+ * method (setAlternativeRelativeMatrixMethod(true)).  The reference fixes the
+ * image at 640 x 480. */
+int mvs_read_icl_camera(const char *path, int32_t width, int32_t height, float *h_K9, float *h_R9, float *h_t3);
+/* PLY point cloud (x y z float, optional red green blue uchar), ASCII or
+ * binary little-endian; replaces the PCL cloud of pclviewer.cpp:1058-1083. */
+int mvs_write_ply(const char *path, const float *h_xyz, const uint8_t *h_rgb, int64_t n, int32_t binary);
+/* The depth colour map of the reference's viewer (PCLViewer::RGBdepthmapColor,
+ * pclviewer.cpp:1084-1115): n gray values -> n RGB triples. */
+void mvs_depth_color(const uint8_t *h_gray, int64_t n, uint8_t *h_rgb);
+
 /* ---- synthetic scenes (no counterpart in the reference) -------------------
  * Ray casts the seeded box scenes that stand in for the reference's datasets
  * (ICL-NUIM, KITTI; reader.cpp, kitti_reader.cpp): an optional room seen

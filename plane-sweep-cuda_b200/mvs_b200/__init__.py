@@ -137,6 +137,9 @@ _sig("mvs_batch_set_poses", C.c_int, _VP, _D, _D, _VP)
 _sig("mvs_batch_run", C.c_int, _VP, _VP)
 _sig("mvs_batch_frame_latency_ms", C.c_int, _VP, _F, _VP)
 _sig("mvs_batch_work_items", C.c_int64, _VP)
+_sig("mvs_read_icl_camera", C.c_int, C.c_char_p, C.c_int32, C.c_int32, _F, _F, _F)
+_sig("mvs_write_ply", C.c_int, C.c_char_p, _F, C.POINTER(C.c_uint8), C.c_int64, C.c_int32)
+_sig("mvs_depth_color", None, C.POINTER(C.c_uint8), C.c_int64, C.POINTER(C.c_uint8))
 _sig("mvs_tvl1_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32)
 _sig("mvs_tvl1_denoise", C.c_int, C.c_int32, C.c_int32, _VP, _VP, C.c_float, C.c_float, C.POINTER(TVL1Params),
      _VP, C.c_size_t, _VP)
@@ -349,6 +352,36 @@ def compute3d(depth, invK9, Rr9, t3, X, Y, Z, stream=None):
     invK9, Rr9, t3 = (_f32(x) for x in (invK9, Rr9, t3))
     check(_L.mvs_compute3d(w, h, _ptr(depth), _fp(invK9), _fp(Rr9), _fp(t3), _ptr(X), _ptr(Y), _ptr(Z),
                            _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# data formats
+# ---------------------------------------------------------------------------
+
+def read_icl_camera(path, width=640, height=480):
+    """(K (1-based, float32 3x3), R (camera->world, 3x3), t (3)) of an ICL-NUIM camera file."""
+    K = np.zeros(9, np.float32)
+    R = np.zeros(9, np.float32)
+    t = np.zeros(3, np.float32)
+    check(_L.mvs_read_icl_camera(str(path).encode(), width, height, _fp(K), _fp(R), _fp(t)))
+    return K.reshape(3, 3), R.reshape(3, 3), t
+
+
+def write_ply(path, xyz, rgb=None, binary=False):
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    c = None
+    if rgb is not None:
+        rgb = np.ascontiguousarray(rgb, np.uint8).reshape(-1, 3)
+        assert len(rgb) == len(xyz)
+        c = rgb.ctypes.data_as(C.POINTER(C.c_uint8))
+    check(_L.mvs_write_ply(str(path).encode(), _fp(xyz), c, len(xyz), int(binary)))
+
+
+def depth_color(gray):
+    g = np.ascontiguousarray(gray, np.uint8).reshape(-1)
+    out = np.empty((g.size, 3), np.uint8)
+    _L.mvs_depth_color(g.ctypes.data_as(C.POINTER(C.c_uint8)), g.size, out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -570,9 +603,17 @@ class FusionVolume:
     def update_p(self, sigma, stream=None):
         check(_L.mvs_fusion_update_p(self.h, sigma, _stream(stream)))
 
-    def iteration(self, depth, K, R, t, threshold, tau, lam, sigma, stream=None):
-        h, w = depth.shape[-2:]
-        check(_L.mvs_fusion_iteration(self.h, _ptr(depth), w, h, _fp(_f32(K)), _fp(_f32(R)), _fp(_f32(t)), threshold,
+    def iteration(self, depth, K, R, t, threshold, tau, lam, sigma, stream=None, shape=None):
+        """One FusionUpdateIteration: ``depth`` a CUDA tensor (H, W), or a raw
+        device pointer (int, e.g. PlaneSweep.getDepthmapDenoisedPtr()) with
+        ``shape`` = (H, W)."""
+        if isinstance(depth, int):
+            h, w = shape
+            dp = C.c_void_p(depth)
+        else:
+            h, w = depth.shape[-2:]
+            dp = _ptr(depth)
+        check(_L.mvs_fusion_iteration(self.h, dp, w, h, _fp(_f32(K)), _fp(_f32(R)), _fp(_f32(t)), threshold,
                                       tau, lam, sigma, _stream(stream)))
 
     def download(self):
