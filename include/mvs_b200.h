@@ -194,6 +194,22 @@ int mvs_tgv2_run_warm(int32_t width, int32_t height, int32_t n_views, const floa
                       double dual_sigma_r, float *d_pq, float *d_r, int32_t *iters_out, double *energy_out, void *d_workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ---- TGV2 towards a sparse depthmap -----------------------------------------
+ * Replaces PlaneSweep::TGVdenoiseFromSparse's chain (planesweep.cpp:596-674):
+ * Anisotropic_diffusion_tensor, then niters x (TGV2_updateP_tensor_weighed on
+ * u, TGV2_updateQ, TGV2_updateU_sparseDepthTensor with v passed as its own
+ * over-relaxation; TGV2_kernels.cu:54-85,340-445), data weight 1 where
+ * d_sparse > 0.  d_depthmap: the start depth (the sweep result), d_sparse: the
+ * sparse depth (0 = none), both in depth units, H*W; d_out = u * zfar.  theta
+ * is accepted for the reference's signature; it only reaches the over-relaxed
+ * u, which the iteration never reads, so it does not change the result. */
+size_t mvs_tgv2_sparse_workspace_bytes(int32_t width, int32_t height);
+
+int mvs_tgv2_sparse(int32_t width, int32_t height, const float *d_ref255, const float *d_depthmap,
+                    const float *d_sparse, float zfar, int32_t niters, double alpha0, double alpha1, double tau,
+                    double sigma, double theta, double beta, double gamma, float *d_out, void *d_workspace,
+                    size_t workspace_bytes, void *stream);
+
 /* ---- TV-L1 depth denoise --------------------------------------------------
  * Replaces PlaneSweep::CudaDenoise's chain (planesweep.cpp:297-379):
  * Anisotropic_diffusion_tensor + denoising_TVL1_calculateP_tensor_weighed +
@@ -289,6 +305,10 @@ int mvs_ps_cuda_denoise(mvs_planesweep *ps, int32_t niters, double lambda, doubl
                         double theta, double beta, double gamma);  /* CudaDenoise */
 int mvs_ps_tgv(mvs_planesweep *ps, int32_t niters, int32_t warps, double lambda, double alpha0, double alpha1,
                double tau, double sigma, double beta, double gamma); /* TGV (u = 1 start) */
+/* TGVdenoiseFromSparse: TGV2 from the last sweep depthmap towards h_sparse
+ * (width*height, 0 = no sample); the result replaces the TGV depthmap. */
+int mvs_ps_tgv_denoise_from_sparse(mvs_planesweep *ps, const float *h_sparse, int32_t niters, double alpha0,
+                                   double alpha1, double tau, double sigma, double theta, double beta, double gamma);
 /* Extension: TGV2 started from the last sweep depthmap (start = 1), from
  * h_u_init (start = 2) or from 1 (start = 0), with an energy tolerance. */
 int mvs_ps_tgv_ext(mvs_planesweep *ps, const mvs_tgv2_params *params, int32_t start, const float *h_u_init,

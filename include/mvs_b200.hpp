@@ -207,6 +207,11 @@ public:
     bool TGV(int argc, char **argv, const unsigned int niters = 30, const unsigned int warps = 15,
              const double lambda = 0.5, const double alpha0 = 2.0, const double alpha1 = 1.5, const double tau = 0.02,
              const double sigma = 1.f, const double beta = 0.f, const double gamma = 1.f);
+    /* TGV2 from the last sweep depthmap towards a sparse depthmap (0 = no
+     * sample); the result is the TGV depthmap (planesweep.cpp:596-674). */
+    bool TGVdenoiseFromSparse(int argc, char **argv, const CamImage<float> &depth, const unsigned int niters,
+                              const double alpha0, const double alpha1, const double tau, const double sigma,
+                              const double theta, const double beta, const double gamma);
     /* Extension: TGV2 from the last sweep depthmap (start = 1), a given
      * depthmap (start = 2) or 1 (start = 0), with an energy tolerance. */
     bool TGVext(const mvs_tgv2_params &p, int start, const CamImage<float> *init = 0, int *iters = 0,

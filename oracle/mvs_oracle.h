@@ -52,6 +52,10 @@ extern "C" {
                                const R *T21, const R *T22, const R *It, const R *Iu,            \
                                const R *u0, const R *u, const R *u1x, const R *u1y,             \
                                double lambda, double alpha0, double alpha1);                    \
+    void orc_tgv_sparse_iteration_##S(int w, int h, const R *T11, const R *T12, const R *T21,    \
+                                      const R *T22, const R *wgt, const R *Ds, R *u, R *vx,     \
+                                      R *vy, R *Px, R *Py, R *Qx, R *Qy, R *Qz, R *Qw,          \
+                                      double alpha0, double alpha1, double tau, double sigma);  \
     void orc_tvl1_denoise_##S(int w, int h, const R *ref255, const R *depth, double znear,      \
                               double zfar, int niters, double lambda, double tau, double sigma, \
                               double theta, double beta, double gamma, R *out);                 \

@@ -440,6 +440,63 @@ double FN(orc_tgv2_energy)(int w, int h, int nview, const R *T11, const R *T12, 
     return alpha1 * e1 + alpha0 * e0 + lambda * ed;
 }
 
+/* ---- TGV2 towards a sparse depthmap: PlaneSweep::TGVdenoiseFromSparse
+ * (planesweep.cpp:596-674).  One iteration of its loop (planesweep.cpp:638-649):
+ * TGV2_updateP_tensor_weighed_kernel (TGV2_kernels.cu:340-365) on u itself,
+ * TGV2_updateQ_kernel (:54-85) and TGV2_updateU_sparseDepthTensor_kernel
+ * (:399-430), each a full-image pass.  The reference passes vxbar / vybar as
+ * both v and its over-relaxation, so v keeps the plain update (the
+ * over-relaxation v + theta (v - v) is v itself); the over-relaxed u it also
+ * writes is never read and is left out. ---- */
+void FN(orc_tgv_sparse_iteration)(int w, int h, const R *T11, const R *T12, const R *T21, const R *T22,
+                                  const R *wgt, const R *Ds, R *u, R *vx, R *vy, R *Px, R *Py, R *Qx, R *Qy,
+                                  R *Qz, R *Qw, double alpha0_, double alpha1_, double tau_, double sigma_)
+{
+    const R alpha0 = (R)alpha0_, alpha1 = (R)alpha1_, tau = (R)tau_, sigma = (R)sigma_;
+    for (int yy = 0; yy < h; ++yy)
+        for (int xx = 0; xx < w; ++xx) {
+            int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
+            double x = u[yy * w + xn] - u[i] - vx[i];
+            double y = u[yn * w + xx] - u[i] - vy[i];
+            double dx = Px[i] + alpha1 * sigma * (T11[i] * x + T12[i] * y);
+            double dy = Py[i] + alpha1 * sigma * (T21[i] * x + T22[i] * y);
+            double d = FMAXR(1, sqrt(dx * dx + dy * dy));
+            Px[i] = (R)(dx / d);
+            Py[i] = (R)(dy / d);
+        }
+    for (int yy = 0; yy < h; ++yy)
+        for (int xx = 0; xx < w; ++xx) {
+            int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
+            R dx_u1x = vx[yy * w + xn] - vx[i];
+            R dy_u1x = vx[yn * w + xx] - vx[i];
+            R dx_u1y = vy[yy * w + xn] - vy[i];
+            R dy_u1y = vy[yn * w + xx] - vy[i];
+            double dx = Qx[i] + alpha0 * sigma * dx_u1x;
+            double dy = Qy[i] + alpha0 * sigma * dy_u1y;
+            double dz = Qz[i] + alpha0 * sigma * (dy_u1x + dx_u1y) / (R)2;
+            double dw = Qw[i] + alpha0 * sigma * (dy_u1x + dx_u1y) / (R)2;
+            double d = FMAXR(1, sqrt(dx * dx + dy * dy + dz * dz + dw * dw));
+            Qx[i] = (R)(dx / d);
+            Qy[i] = (R)(dy / d);
+            Qz[i] = (R)(dz / d);
+            Qw[i] = (R)(dw / d);
+        }
+    for (int yy = 0; yy < h; ++yy)
+        for (int xx = 0; xx < w; ++xx) {
+            int i = yy * w + xx, xp = xx - 1 > 0 ? xx - 1 : 0, yp = yy - 1 > 0 ? yy - 1 : 0;
+            R c_px = Px[i], c_py = Py[i], xp_px = Px[yy * w + xp], yp_px = Px[yp * w + xx],
+              xp_py = Py[yy * w + xp], yp_py = Py[yp * w + xx];
+            u[i] = (u[i] + tau * (alpha1 * (T11[i] * (c_px - xp_px) + T12[i] * (c_py - xp_py) +
+                                            T21[i] * (c_px - yp_px) + T22[i] * (c_py - yp_py)) +
+                                  wgt[i] * Ds[i])) /
+                   (1 + tau * wgt[i]);
+            vx[i] = vx[i] - tau * (-alpha1 * (T11[i] * c_px + T12[i] * c_py) -
+                                   alpha0 * (Qx[i] - Qx[yy * w + xp] + Qz[i] - Qz[yp * w + xx]));
+            vy[i] = vy[i] - tau * (-alpha1 * (T21[i] * c_px + T22[i] * c_py) -
+                                   alpha0 * (Qz[i] - Qz[yy * w + xp] + Qy[i] - Qy[yp * w + xx]));
+        }
+}
+
 /* ---- TV-L1 depth denoise: PlaneSweep::CudaDenoise (planesweep.cpp:297-379) ---- */
 
 void FN(orc_tvl1_denoise)(int w, int h, const R *ref255, const R *depth, double znear_, double zfar_, int niters,

@@ -84,6 +84,7 @@ def _declare_oracle(L):
         getattr(L, f"orc_tgv2_iteration_{S}").argtypes = ([C.c_int] * 3 + [P] * 21 + [C.c_double] * 5)
         getattr(L, f"orc_tgv2_energy_{S}").argtypes = [C.c_int] * 3 + [P] * 10 + [C.c_double] * 3
         getattr(L, f"orc_tgv2_energy_{S}").restype = C.c_double
+        getattr(L, f"orc_tgv_sparse_iteration_{S}").argtypes = [C.c_int] * 2 + [P] * 15 + [C.c_double] * 4
         getattr(L, f"orc_tvl1_denoise_{S}").argtypes = ([C.c_int, C.c_int, P, P, C.c_double, C.c_double, C.c_int]
                                                         + [C.c_double] * 6 + [P])
         getattr(L, f"orc_fusion_histogram_{S}").argtypes = [C.c_int] * 4 + [_F, _F, _U16, _F, C.c_int, C.c_int,
@@ -99,6 +100,8 @@ def _declare_oracle(L):
 
 
 def _declare_ref(L):
+    L.ref_tgv_sparse.restype = C.c_double
+    L.ref_tgv_sparse.argtypes = [C.c_int, C.c_int, _F, _F, _F, C.c_float, C.c_int] + [C.c_double] * 7 + [_F]
     L.ref_sweep.argtypes = [C.c_int, C.c_int, _F, _F, C.c_int, _F, _F, _F, _F, _F, C.c_int, _F, C.c_int,
                             C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, _F, _F, _F]
     L.ref_sweep.restype = C.c_double
@@ -275,6 +278,19 @@ def ref_gpu_tgv(ref, srcs, K_1based, Rref, tref, src_poses, niters, warps, u_ini
     return out, ms
 
 
+def ref_tgv_sparse(ref, depthmap, sparse, zfar, niters, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, theta=1.0,
+                   beta=0.0, gamma=1.0):
+    """The reference's PlaneSweep::TGVdenoiseFromSparse on the CPU (its own kernels)."""
+    L = ref_lib()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref/libmvs_ref.so not built")
+    h, w = ref.shape
+    out = np.zeros((h, w), np.float32)
+    L.ref_tgv_sparse(w, h, _fp(_f32(ref)), _fp(_f32(depthmap)), _fp(_f32(sparse)), float(zfar), niters, alpha0, alpha1,
+                     tau, sigma, theta, beta, gamma, _fp(out))
+    return out
+
+
 def labels_from_depth(vdepth, planes):
     """Per-view plane index from the reference's stored depth (0 -> -1)."""
     planes = np.asarray(planes, np.float32)
@@ -396,6 +412,34 @@ def tgv2(ref255, srcs255, K_1based, Rref, tref, src_poses, niters=30, warps=15, 
                 done = True
                 break
     return S.u.copy(), total, energies
+
+
+def tgv_sparse(ref255, depthmap, sparse, zfar, niters, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, theta=1.0,
+               beta=0.0, gamma=1.0, precision="f64", T=None):
+    """PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674) over the C
+    restatement: weights = (sparse > 0), Ds = sparse * (1/zfar), u = depthmap *
+    (1/zfar), the anisotropic tensor of ref/255, ``niters`` iterations, u * zfar.
+    ``theta`` only reaches the over-relaxed u, which nothing reads.  ``T``
+    (T11, T12, T21, T22) replaces the tensor when given."""
+    L = oracle_lib()
+    dt = np.float32 if precision == "f32" else np.float64
+    P = _fp if precision == "f32" else _dp
+    h, w = depthmap.shape
+    one = dt(1)
+    inv_zfar = dt(np.float32(1) / np.float32(zfar)) if precision == "f32" else 1.0 / zfar
+    sp = np.asarray(sparse, dt)
+    wgt = np.ascontiguousarray(np.where(sp > 0, one, dt(0)), dt)
+    Ds = np.ascontiguousarray(sp * inv_zfar, dt)
+    u = np.ascontiguousarray(np.asarray(depthmap, dt) * inv_zfar, dt)
+    scale = np.float32(1) / np.float32(255) if precision == "f32" else 1.0 / 255.0
+    if T is None:
+        T = tensor(np.ascontiguousarray(np.asarray(ref255, dt) * dt(scale), dt), beta, gamma, precision)
+    T = [np.ascontiguousarray(t, dt) for t in T]
+    st = [np.zeros((h, w), dt) for _ in range(8)]   # vx, vy, Px, Py, Qx, Qy, Qz, Qw
+    fn = getattr(L, f"orc_tgv_sparse_iteration_{precision}")
+    for _ in range(niters):
+        fn(w, h, *[P(t) for t in T], P(wgt), P(Ds), P(u), *[P(a) for a in st], alpha0, alpha1, tau, sigma)
+    return (u * dt(zfar)).astype(dt)
 
 
 def ref_tgv(ref255, srcs255, K_1based, Rref, tref, src_poses, niters=30, warps=15, lam=0.5, alpha0=2.0,

@@ -268,6 +268,43 @@ double ref_tgv(int w, int h, const float *refimg, const float *srcs, int nsrc,
     return now() - t0;
 }
 
+/* PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674): TGV2 of the
+ * sweep's depthmap towards a sparse depth (weight 1 where the sparse depth is
+ * positive), both divided by zfar.  The call at planesweep.cpp:645 hands the
+ * update kernel vxbar / vybar as both v and its over-relaxation, and the P
+ * step reads u itself (d_depthmap) rather than ubar: replayed as written. */
+double ref_tgv_sparse(int w, int h, const float *refimg, const float *depthmap, const float *sparse, float zfar,
+                      int niters, double alpha0, double alpha1, double tau, double sigma, double theta, double beta,
+                      double gamma, float *out)
+{
+    const double t0 = now();
+    const size_t n = (size_t)w * h;
+    Grid g(w, h);
+    const dim3 &B = g.blocks, &T = g.threads;
+    img px(n, 0.f), py(n, 0.f), qx(n, 0.f), qy(n, 0.f), qz(n, 0.f), qw(n, 0.f), ubar(depthmap, depthmap + n),
+        vxbar(n, 0.f), vybar(n, 0.f), weights(n, 0.f), Ds(sparse, sparse + n), ref(refimg, refimg + n), T1(n, 0.f),
+        T2(n, 0.f), T3(n, 0.f), T4(n, 0.f);
+    calculateWeights_sparseDepth(weights.data(), Ds.data(), w, h, B, T);
+    element_scale(Ds.data(), 1.f / zfar, w, h, B, T);
+    element_scale(ubar.data(), 1.f / zfar, w, h, B, T);
+    img u(ubar);   /* d_depthmap = ubar */
+    element_scale(ref.data(), 1.f / 255.f, w, h, B, T);
+    Anisotropic_diffusion_tensor(T1.data(), T2.data(), T3.data(), T4.data(), ref.data(), beta, gamma, w, h, B, T);
+    for (int i = 0; i < niters; i++) {
+        TGV2_updateP_tensor_weighed(px.data(), py.data(), T1.data(), T2.data(), T3.data(), T4.data(), u.data(),
+                                    vxbar.data(), vybar.data(), alpha1, sigma, w, h, B, T);
+        TGV2_updateQ(qx.data(), qy.data(), qz.data(), qw.data(), vxbar.data(), vybar.data(), alpha0, sigma, w, h, B,
+                     T);
+        TGV2_updateU_sparseDepthTensor(u.data(), vxbar.data(), vybar.data(), ubar.data(), vxbar.data(), vybar.data(),
+                                       T1.data(), T2.data(), T3.data(), T4.data(), px.data(), py.data(), qx.data(),
+                                       qy.data(), qz.data(), qw.data(), weights.data(), Ds.data(), alpha0, alpha1, tau,
+                                       theta, w, h, B, T);
+    }
+    element_scale(u.data(), zfar, w, h, B, T);
+    std::memcpy(out, u.data(), n * sizeof(float));
+    return now() - t0;
+}
+
 /* PlaneSweep::CudaDenoise (planesweep.cpp:297-379): TV-L1 with the tensor
  * weighted dual step, on a depthmap normalised to [0,1] over [znear, zfar]. */
 double ref_tvl1_denoise(int w, int h, const float *refimg, const float *depth, float znear, float zfar,

@@ -49,6 +49,10 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
              const float *Rrel, const float *trel, const mvs_tgv2_params *prm, int u_from_input, float u_init,
              float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st,
              const TGV2Warm *warm = nullptr);
+size_t tgv2_sparse_workspace_bytes(int w, int h);
+int tgv2_sparse_run(int w, int h, const float *ref255, const float *depthmap, const float *sparse, float zfar,
+                    int niters, double alpha0, double alpha1, double tau, double sigma, double beta, double gamma,
+                    float *out, void *ws, cudaStream_t st);
 // tvl1.cu
 size_t tvl1_workspace_bytes(int w, int h);
 int tvl1_run(int w, int h, const float *ref255, float *depth, float znear, float zfar, const mvs_tvl1_params *prm,
@@ -276,6 +280,29 @@ int mvs_tgv2_run_warm(int32_t w, int32_t h, int32_t V, const float *ref255, cons
                       (cudaStream_t)stream, &warm);
     if (iters_out) *iters_out = it;
     return rc;
+}
+
+size_t mvs_tgv2_sparse_workspace_bytes(int32_t w, int32_t h)
+{
+    if (w <= 0 || h <= 0) return 0;
+    return tgv2_sparse_workspace_bytes(w, h);
+}
+
+int mvs_tgv2_sparse(int32_t w, int32_t h, const float *ref255, const float *depthmap, const float *sparse, float zfar,
+                    int32_t niters, double alpha0, double alpha1, double tau, double sigma, double theta, double beta,
+                    double gamma, float *out, void *ws, size_t ws_bytes, void *stream)
+{
+    clear_error();
+    (void)theta;   // enters only the over-relaxed u, which the iteration never reads
+    if (w < 1 || h < 1) return set_error(MVS_ERR_ARG, "bad size %dx%d", w, h);
+    if ((int64_t)w * h > INT32_MAX) return set_error(MVS_ERR_ARG, "image too large");
+    if (!ref255 || !depthmap || !sparse || !out) return set_error(MVS_ERR_ARG, "null pointer");
+    if (niters < 0) return set_error(MVS_ERR_ARG, "negative iteration count");
+    if (!(zfar != 0.f)) return set_error(MVS_ERR_ARG, "zfar == 0");
+    const size_t need = tgv2_sparse_workspace_bytes(w, h);
+    if (!ws || ws_bytes < need) return set_error(MVS_ERR_ARG, "workspace of %zu bytes needed", need);
+    return tgv2_sparse_run(w, h, ref255, depthmap, sparse, zfar, niters, alpha0, alpha1, tau, sigma, beta, gamma, out,
+                           ws, (cudaStream_t)stream);
 }
 
 // ---- TV-L1 ------------------------------------------------------------------------------

@@ -380,6 +380,47 @@ bool PlaneSweep::TGVext(const mvs_tgv2_params &prm, int start, const CamImage<fl
     return true;
 }
 
+bool PlaneSweep::TGVdenoiseFromSparse(int, char **, const CamImage<float> &depth, const unsigned int niters,
+                                      const double alpha0, const double alpha1, const double tau, const double sigma,
+                                      const double theta, const double beta, const double gamma)
+{
+    PlaneSweepImpl &I = *impl;
+    const int w = (int)HostRef.width(), h = (int)HostRef.height();
+    const size_t n = (size_t)w * h;
+    if (!depthavailable || (int)depthmap.width() != w || (int)depthmap.height() != h) {
+        mvs::set_error(MVS_ERR_STATE, "TGVdenoiseFromSparse needs a depthmap from RunAlgorithm");
+        return false;
+    }
+    if ((int)depth.width() != w || (int)depth.height() != h) {
+        mvs::set_error(MVS_ERR_ARG, "sparse depthmap of the wrong size");
+        return false;
+    }
+    depthmapTGV.reset(w, h);
+    depthmap8uTGV.reset(w, h);
+    if (I.ref.ensure(n * 4) || I.tvu.ensure(n * 4) || I.tvsrc.ensure(n * 4) ||
+        I.tvws.ensure(std::max(mvs_tgv2_sparse_workspace_bytes(w, h), mvs_tvl1_workspace_bytes(w, h))))
+        return false;
+    cudaStream_t st = 0;
+    if (cudaMemcpyAsync(I.ref.p, HostRef.data(), n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(I.tvsrc.p, depth.data(), n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        mvs::set_error(MVS_ERR_CUDA, "TGVdenoiseFromSparse copy: %s", cudaGetErrorString(cudaGetLastError()));
+        return false;
+    }
+    cudaEventRecord(I.e0, st);
+    if (mvs_tgv2_sparse(w, h, I.ref.as<float>(), I.depth.as<float>(), I.tvsrc.as<float>(), zfar, (int)niters, alpha0,
+                        alpha1, tau, sigma, theta, beta, gamma, I.tvu.as<float>(), I.tvws.p, I.tvws.bytes, st))
+        return false;
+    cudaEventRecord(I.e1, st);
+    if (cudaMemcpyAsync(depthmapTGV.data(), I.tvu.p, n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        mvs::set_error(MVS_ERR_CUDA, "TGVdenoiseFromSparse: %s", cudaGetErrorString(cudaGetLastError()));
+        return false;
+    }
+    cudaEventElapsedTime(&lastms, I.e0, I.e1);
+    ConvertDepthtoUChar(depthmapTGV, depthmap8uTGV);
+    return true;
+}
+
 bool PlaneSweep::TGV(int, char **, const unsigned int niters, const unsigned int warps, const double lambda,
                      const double alpha0, const double alpha1, const double tau, const double sigma, const double beta,
                      const double gamma)
@@ -588,6 +629,20 @@ int mvs_ps_tgv(mvs_planesweep *ps, int32_t niters, int32_t warps, double lambda,
     if (niters < 0 || warps < 0) return mvs::set_error(MVS_ERR_ARG, "negative iteration count");
     return ps->ps.TGV(0, nullptr, niters, warps, lambda, alpha0, alpha1, tau, sigma, beta, gamma) ? MVS_OK
                                                                                                   : MVS_ERR_STATE;
+}
+
+int mvs_ps_tgv_denoise_from_sparse(mvs_planesweep *ps, const float *h_sparse, int32_t niters, double alpha0,
+                                   double alpha1, double tau, double sigma, double theta, double beta, double gamma)
+{
+    PS_CHECK(ps);
+    if (!h_sparse) return mvs::set_error(MVS_ERR_ARG, "null sparse depthmap");
+    if (niters < 0) return mvs::set_error(MVS_ERR_ARG, "negative iteration count");
+    CamImage<float> sp;
+    sp.reset(ps->ps.HostRef.width(), ps->ps.HostRef.height());
+    memcpy(sp.data(), h_sparse, sizeof(float) * sp.elements());
+    return ps->ps.TGVdenoiseFromSparse(0, nullptr, sp, niters, alpha0, alpha1, tau, sigma, theta, beta, gamma)
+               ? MVS_OK
+               : MVS_ERR_STATE;
 }
 
 int mvs_ps_tgv_ext(mvs_planesweep *ps, const mvs_tgv2_params *p, int32_t start, const float *u_init, int32_t *iters,

@@ -814,13 +814,15 @@ __global__ void wta_finish_kernel(const unsigned long long *__restrict__ wta, co
 }
 
 // WTA argmin over a stored BF16 cost volume [P][n]: the HBM-bound pass.
-// A block owns 32 groups of 8 consecutive pixels; its 8 warps split the planes
-// into 8 contiguous slices, each lane reading one 16-byte group per plane (a
-// warp reads 512 contiguous bytes per plane).  The slices' minima are merged
+// A block owns 32 groups of 8 consecutive pixels; its WTA_WARPS warps split the
+// planes into contiguous slices, each lane reading one 16-byte group per plane
+// (a warp reads 512 contiguous bytes per plane).  The slices' minima are merged
 // in plane order through shared memory, so ties keep the earliest plane.
-constexpr int WTA_WARPS = 8;
+// 4 warps per block: the 1200 blocks of a 640x480 frame are then all resident
+// at once (16 per SM) instead of 1184 plus a 16-block second wave.
+constexpr int WTA_WARPS = 4;
 
-__global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restrict__ cost, const float *__restrict__ depths,
+__global__ void __launch_bounds__(32 * WTA_WARPS) wta_volume_kernel(const uint16_t *__restrict__ cost, const float *__restrict__ depths,
                                                         int n, int P, float zfar, float *__restrict__ depth,
                                                         int32_t *__restrict__ labels, float *__restrict__ best)
 {
@@ -838,7 +840,7 @@ __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restr
     for (int j = 0; j < 8; ++j) key[j] = 0xffffffffu;
     if (g < n8) {
         const uint4 *col = reinterpret_cast<const uint4 *>(cost) + g;
-#pragma unroll 4
+#pragma unroll 8
         for (int p = p0; p < p1; ++p) {
             const uint4 q = __ldcs(col + (size_t)p * n8);
             const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
@@ -852,19 +854,21 @@ __global__ void __launch_bounds__(256) wta_volume_kernel(const uint16_t *__restr
 #pragma unroll
     for (int j = 0; j < 8; ++j) sk[wid][lane][j] = key[j];
     __syncthreads();
-    // thread t finalises pixel j = t & 7 of group t >> 3
-    const int gl = threadIdx.x >> 3, j = threadIdx.x & 7;
-    const int gg = blockIdx.x * 32 + gl;
-    if (gg >= n8) return;
-    uint32_t kmin = 0xffffffffu;
+    // each of the block's 256 (group, pixel) results is finalised by one thread
+    for (int q = threadIdx.x; q < 32 * 8; q += 32 * WTA_WARPS) {
+        const int gl = q >> 3, j = q & 7;
+        const int gg = blockIdx.x * 32 + gl;
+        if (gg >= n8) continue;
+        uint32_t kmin = 0xffffffffu;
 #pragma unroll
-    for (int k = 0; k < WTA_WARPS; ++k) kmin = min(kmin, sk[k][gl][j]);
-    const int l = kmin == 0xffffffffu ? -1 : (int)(kmin & 0xffffu);
-    const float c = l >= 0 ? bf2f((uint16_t)(kmin >> 16)) : 3.f;
-    const int px = 8 * gg + j;
-    depth[px] = l >= 0 ? ldg(depths + l) : zfar;
-    if (labels) labels[px] = l;
-    if (best) best[px] = c;
+        for (int k = 0; k < WTA_WARPS; ++k) kmin = min(kmin, sk[k][gl][j]);
+        const int l = kmin == 0xffffffffu ? -1 : (int)(kmin & 0xffffu);
+        const float c = l >= 0 ? bf2f((uint16_t)(kmin >> 16)) : 3.f;
+        const int px = 8 * gg + j;
+        depth[px] = l >= 0 ? ldg(depths + l) : zfar;
+        if (labels) labels[px] = l;
+        if (best) best[px] = c;
+    }
 }
 
 // FP64 homographies: H = K (Rrel + trel e3^T / d) K^-1, H /= H22, for one
@@ -1180,8 +1184,8 @@ int sweep_wta_volume(const uint16_t *cost, const float *depths, int n, int P, fl
                      int32_t *labels, float *best, void *stream)
 {
     if (n % 8) return set_error(MVS_ERR_ARG, "WTA over a cost volume needs W*H divisible by 8");
-    wta_volume_kernel<<<ceil_div(n / 8, 32), 256, 0, (cudaStream_t)stream>>>(cost, depths, n, P, zfar, depth, labels,
-                                                                           best);
+    wta_volume_kernel<<<ceil_div(n / 8, 32), 32 * WTA_WARPS, 0, (cudaStream_t)stream>>>(cost, depths, n, P, zfar,
+                                                                                       depth, labels, best);
     return check_launch("wta_volume_kernel");
 }
 

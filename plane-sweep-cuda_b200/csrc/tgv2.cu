@@ -942,7 +942,217 @@ int persist_tile_height(int w, int h, int V, int sms, size_t smem_limit)
     return th;
 }
 
+// ---- TGV2 towards a sparse depth (PlaneSweep::TGVdenoiseFromSparse) ----------------
+//
+// planesweep.cpp:596-674 with TGV2_kernels.cu:340-445: P from u itself (the
+// call passes d_depthmap, not ubar), Q from v, and the update of
+// TGV2_updateU_sparseDepthTensor_kernel, whose call at planesweep.cpp:645
+// passes vxbar / vybar as both v and its over-relaxation, so the in-place
+// update leaves vbar == v.  ubar is written there but never read (P takes u),
+// so it does not change the result and is not kept here; neither is theta,
+// which only enters ubar.  One fused launch per iteration, P and Q recomputed
+// on the left / top halo as in iteration_kernel; u, v, p, q are
+// double-buffered because neighbouring CTAs read them.
+
+struct SparseBufs {
+    const float *T11, *T12, *T22, *wgt, *Ds;
+    const float *u_in, *vx_in, *vy_in, *Px_in, *Py_in, *Qx_in, *Qy_in, *Qz_in;
+    float *u_out, *vx_out, *vy_out, *Px_out, *Py_out, *Qx_out, *Qy_out, *Qz_out;
+    int w, h;
+    float alpha0, alpha1, tau, sigma;
+};
+
+__global__ void __launch_bounds__(TX *TY) sparse_iteration_kernel(SparseBufs b)
+{
+    __shared__ float sU[TY + 2][TX + 2], sVX[TY + 2][TX + 2], sVY[TY + 2][TX + 2];
+    __shared__ float sPx[TY + 1][TX + 1], sPy[TY + 1][TX + 1];
+    __shared__ float sQx[TY + 1][TX + 1], sQy[TY + 1][TX + 1], sQz[TY + 1][TX + 1];
+    const int w = b.w, h = b.h;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int tid = threadIdx.y * TX + threadIdx.x;
+    for (int k = tid; k < (TX + 2) * (TY + 2); k += TX * TY) {
+        const int ry = k / (TX + 2), rx = k % (TX + 2);
+        const int px = min(max(x0 - 1 + rx, 0), w - 1), py = min(max(y0 - 1 + ry, 0), h - 1);
+        const int j = py * w + px;
+        sU[ry][rx] = b.u_in[j];
+        sVX[ry][rx] = b.vx_in[j];
+        sVY[ry][rx] = b.vy_in[j];
+    }
+    __syncthreads();
+    // TGV2_updateP_tensor_weighed (TGV2_kernels.cu:340-365) on u and v, TGV2_updateQ (:54-85) on v
+    const float a1s = b.alpha1 * b.sigma, a0s = b.alpha0 * b.sigma;
+    for (int k = tid; k < (TX + 1) * (TY + 1); k += TX * TY) {
+        const int ry = k / (TX + 1), rx = k % (TX + 1);
+        const int px = x0 - 1 + rx, py = y0 - 1 + ry;
+        if (px < 0 || py < 0 || px >= w || py >= h) continue;
+        const int j = py * w + px;
+        const int nx = px + 1 <= w - 1 ? rx + 1 : rx, ny = py + 1 <= h - 1 ? ry + 1 : ry;
+        {
+            const double xg = sU[ry][nx] - sU[ry][rx] - sVX[ry][rx];
+            const double yg = sU[ny][rx] - sU[ry][rx] - sVY[ry][rx];
+            const double c11 = b.T11[j], c12 = b.T12[j], c22 = b.T22[j];
+            double dx = (double)b.Px_in[j] + (double)a1s * (c11 * xg + c12 * yg);
+            double dy = (double)b.Py_in[j] + (double)a1s * (c12 * xg + c22 * yg);
+            proj2(dx * dx + dy * dy, dx, dy);
+            sPx[ry][rx] = (float)dx;
+            sPy[ry][rx] = (float)dy;
+        }
+        {
+            const float dx_u1x = sVX[ry][nx] - sVX[ry][rx];
+            const float dy_u1x = sVX[ny][rx] - sVX[ry][rx];
+            const float dx_u1y = sVY[ry][nx] - sVY[ry][rx];
+            const float dy_u1y = sVY[ny][rx] - sVY[ry][rx];
+            double dx = b.Qx_in[j] + a0s * dx_u1x;
+            double dy = b.Qy_in[j] + a0s * dy_u1y;
+            double dz = b.Qz_in[j] + a0s * (dy_u1x + dx_u1y) / 2.0f;
+            proj3(dx * dx + dy * dy + dz * dz + dz * dz, dx, dy, dz);
+            sQx[ry][rx] = (float)dx;
+            sQy[ry][rx] = (float)dy;
+            sQz[ry][rx] = (float)dz;
+        }
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int i = y * w + x, lx = threadIdx.x + 1, ly = threadIdx.y + 1;
+    const int lxp = x > 0 ? lx - 1 : lx, lyp = y > 0 ? ly - 1 : ly;
+    // TGV2_updateU_sparseDepthTensor_kernel (TGV2_kernels.cu:399-430)
+    const float t11 = b.T11[i], t12 = b.T12[i], t22 = b.T22[i], wi = b.wgt[i];
+    const float c_px = sPx[ly][lx], c_py = sPy[ly][lx];
+    const float xp_px = sPx[ly][lxp], yp_px = sPx[lyp][lx];
+    const float xp_py = sPy[ly][lxp], yp_py = sPy[lyp][lx];
+    const float uold = sU[ly][lx];
+    const float unew = (uold + b.tau * (b.alpha1 * (t11 * (c_px - xp_px) + t12 * (c_py - xp_py) +
+                                                    t12 * (c_px - yp_px) + t22 * (c_py - yp_py)) +
+                                        wi * b.Ds[i])) /
+                       (1 + b.tau * wi);
+    const float qx = sQx[ly][lx], qy = sQy[ly][lx], qz = sQz[ly][lx];
+    const float vxn = sVX[ly][lx] - b.tau * (-b.alpha1 * (t11 * c_px + t12 * c_py) -
+                                             b.alpha0 * (qx - sQx[ly][lxp] + qz - sQz[lyp][lx]));
+    const float vyn = sVY[ly][lx] - b.tau * (-b.alpha1 * (t12 * c_px + t22 * c_py) -
+                                             b.alpha0 * (qz - sQz[ly][lxp] + qy - sQy[lyp][lx]));
+    b.u_out[i] = unew;
+    b.vx_out[i] = vxn;   // v and its over-relaxation are the same array in the reference
+    b.vy_out[i] = vyn;
+    b.Px_out[i] = c_px;
+    b.Py_out[i] = c_py;
+    b.Qx_out[i] = qx;
+    b.Qy_out[i] = qy;
+    b.Qz_out[i] = qz;
+}
+
+// setup: weights (calculateWeights_sparseDepth_kernel, TGV2_kernels.cu:432-445),
+// Ds / zfar, u = depthmap / zfar (element_scale: x * (1.f / zfar)), the other
+// state at zero
+__global__ void sparse_setup_kernel(const float *__restrict__ depthmap, const float *__restrict__ sparse, int n,
+                                    float inv_zfar, float *__restrict__ wgt, float *__restrict__ Ds,
+                                    float *__restrict__ u, float *__restrict__ vx,
+                                    float *__restrict__ vy, float *__restrict__ Px, float *__restrict__ Py,
+                                    float *__restrict__ Qx, float *__restrict__ Qy, float *__restrict__ Qz)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float s = sparse[i];
+        wgt[i] = s > 0 ? 1.f : 0.f;
+        Ds[i] = s * inv_zfar;
+        u[i] = depthmap[i] * inv_zfar;
+        vx[i] = vy[i] = Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
+    }
+}
+
+__global__ void scale_kernel(const float *__restrict__ in, int n, float s, float *__restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = in[i] * s;
+}
+
+struct SparseLayout {
+    float *ref01, *T11, *T12, *T22, *wgt, *Ds, *u[2], *vx[2], *vy[2], *Px[2], *Py[2], *Qx[2], *Qy[2], *Qz[2];
+    size_t bytes;
+};
+
+SparseLayout sparse_layout(void *base, int w, int h)
+{
+    SparseLayout L{};
+    const size_t n = (size_t)w * h;
+    char *p = (char *)base;
+    size_t off = 0;
+    auto take = [&]() {
+        float *q = (float *)(p + off);
+        off += ((n * sizeof(float) + 255) / 256) * 256;
+        return q;
+    };
+    L.ref01 = take();
+    L.T11 = take();
+    L.T12 = take();
+    L.T22 = take();
+    L.wgt = take();
+    L.Ds = take();
+    for (int k = 0; k < 2; ++k) {
+        L.u[k] = take();
+        L.vx[k] = take();
+        L.vy[k] = take();
+        L.Px[k] = take();
+        L.Py[k] = take();
+        L.Qx[k] = take();
+        L.Qy[k] = take();
+        L.Qz[k] = take();
+    }
+    L.bytes = off;
+    return L;
+}
+
 }  // namespace
+
+size_t tgv2_sparse_workspace_bytes(int w, int h) { return sparse_layout(nullptr, w, h).bytes; }
+
+int tgv2_sparse_run(int w, int h, const float *ref255, const float *depthmap, const float *sparse, float zfar,
+                    int niters, double alpha0, double alpha1, double tau, double sigma, double beta, double gamma,
+                    float *out, void *ws, cudaStream_t st)
+{
+    SparseLayout L = sparse_layout(ws, w, h);
+    const int n = w * h;
+    const dim3 b2(32, 8), g2(ceil_div(w, 32), ceil_div(h, 8));
+    const int eg = min(ceil_div(n, 256), 8 * kSMs);
+    // the reference passes its double parameters to float kernel arguments
+    tensor_kernel<<<g2, b2, 0, st>>>(ref255, w, h, (float)beta, (float)gamma, L.ref01, L.T11, L.T12, L.T22);
+    sparse_setup_kernel<<<eg, 256, 0, st>>>(depthmap, sparse, n, 1.f / zfar, L.wgt, L.Ds, L.u[0], L.vx[0],
+                                           L.vy[0], L.Px[0], L.Py[0], L.Qx[0], L.Qy[0], L.Qz[0]);
+    SparseBufs b;
+    b.T11 = L.T11;
+    b.T12 = L.T12;
+    b.T22 = L.T22;
+    b.wgt = L.wgt;
+    b.Ds = L.Ds;
+    b.w = w;
+    b.h = h;
+    b.alpha0 = (float)alpha0;
+    b.alpha1 = (float)alpha1;
+    b.tau = (float)tau;
+    b.sigma = (float)sigma;
+    int cur = 0;
+    const dim3 gi(ceil_div(w, TX), ceil_div(h, TY)), bi(TX, TY);
+    for (int it = 0; it < niters; ++it) {
+        b.u_in = L.u[cur];
+        b.vx_in = L.vx[cur];
+        b.vy_in = L.vy[cur];
+        b.Px_in = L.Px[cur];
+        b.Py_in = L.Py[cur];
+        b.Qx_in = L.Qx[cur];
+        b.Qy_in = L.Qy[cur];
+        b.Qz_in = L.Qz[cur];
+        b.u_out = L.u[cur ^ 1];
+        b.vx_out = L.vx[cur ^ 1];
+        b.vy_out = L.vy[cur ^ 1];
+        b.Px_out = L.Px[cur ^ 1];
+        b.Py_out = L.Py[cur ^ 1];
+        b.Qx_out = L.Qx[cur ^ 1];
+        b.Qy_out = L.Qy[cur ^ 1];
+        b.Qz_out = L.Qz[cur ^ 1];
+        sparse_iteration_kernel<<<gi, bi, 0, st>>>(b);
+        cur ^= 1;
+    }
+    scale_kernel<<<eg, 256, 0, st>>>(L.u[cur], n, zfar, out);
+    return check_launch("tgv2 sparse");
+}
 
 size_t tgv2_workspace_bytes(int w, int h, int V) { return layout(nullptr, w, h, V).bytes; }
 

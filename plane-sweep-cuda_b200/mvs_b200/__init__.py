@@ -140,6 +140,9 @@ _sig("mvs_batch_work_items", C.c_int64, _VP)
 _sig("mvs_read_icl_camera", C.c_int, C.c_char_p, C.c_int32, C.c_int32, _F, _F, _F)
 _sig("mvs_write_ply", C.c_int, C.c_char_p, _F, C.POINTER(C.c_uint8), C.c_int64, C.c_int32)
 _sig("mvs_depth_color", None, C.POINTER(C.c_uint8), C.c_int64, C.POINTER(C.c_uint8))
+_sig("mvs_tgv2_sparse_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32)
+_sig("mvs_tgv2_sparse", C.c_int, C.c_int32, C.c_int32, _VP, _VP, _VP, C.c_float, C.c_int32, *([C.c_double] * 7), _VP,
+     _VP, C.c_size_t, _VP)
 _sig("mvs_tvl1_workspace_bytes", C.c_size_t, C.c_int32, C.c_int32)
 _sig("mvs_tvl1_denoise", C.c_int, C.c_int32, C.c_int32, _VP, _VP, C.c_float, C.c_float, C.POINTER(TVL1Params),
      _VP, C.c_size_t, _VP)
@@ -175,6 +178,7 @@ _sig("mvs_ps_set_sweep_options", C.c_int, _VP, C.c_int32, C.c_int32, C.c_int32)
 _sig("mvs_ps_run_algorithm", C.c_int, _VP)
 _sig("mvs_ps_cuda_denoise", C.c_int, _VP, C.c_int32, *([C.c_double] * 6))
 _sig("mvs_ps_tgv", C.c_int, _VP, C.c_int32, C.c_int32, *([C.c_double] * 7))
+_sig("mvs_ps_tgv_denoise_from_sparse", C.c_int, _VP, _F, C.c_int32, *([C.c_double] * 7))
 _sig("mvs_ps_tgv_ext", C.c_int, _VP, C.POINTER(TGV2Params), C.c_int32, _F, _I32, _D)
 _sig("mvs_ps_get_size", C.c_int, _VP, _I32, _I32)
 for _n in ("depthmap", "depthmap_denoised", "depthmap_tgv"):
@@ -331,6 +335,21 @@ def render_scene(scene_desc, invK, R, center, width, height, gray255, depth, str
 
 def tgv2_workspace_bytes(w, h, V):
     return int(_L.mvs_tgv2_workspace_bytes(w, h, V))
+
+
+def tgv2_sparse_workspace_bytes(w, h):
+    return int(_L.mvs_tgv2_sparse_workspace_bytes(w, h))
+
+
+def tgv2_sparse(ref255, depthmap, sparse, zfar, out, workspace, niters, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0,
+                theta=1.0, beta=0.0, gamma=1.0, stream=None):
+    """TGV2 from ``depthmap`` towards ``sparse`` (0 = no sample), all device
+    float32 H x W; ``out`` receives the result (PlaneSweep::TGVdenoiseFromSparse,
+    planesweep.cpp:596-674)."""
+    h, w = depthmap.shape[-2:]
+    check(_L.mvs_tgv2_sparse(w, h, _ptr(ref255), _ptr(depthmap), _ptr(sparse), zfar, niters, alpha0, alpha1, tau,
+                             sigma, theta, beta, gamma, _ptr(out), _ptr(workspace),
+                             workspace.numel() * workspace.element_size(), _stream(stream)))
 
 
 def tvl1_params(niters=100, lam=0.3, tau=0.02, sigma=6.0, theta=1.0, beta=0.0, gamma=1.0):
@@ -719,6 +738,14 @@ class PlaneSweep:
 
     def TGV(self, niters=30, warps=15, lam=0.5, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0):
         check(_L.mvs_ps_tgv(self.h, niters, warps, lam, alpha0, alpha1, tau, sigma, beta, gamma))
+
+    def TGVdenoiseFromSparse(self, depth, niters, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, theta=1.0, beta=0.0,
+                             gamma=1.0):
+        sp = _f32(depth)
+        if sp.shape != self.shape:
+            raise ValueError(f"sparse depthmap shape {sp.shape} != {self.shape}")
+        check(_L.mvs_ps_tgv_denoise_from_sparse(self.h, _fp(sp), niters, alpha0, alpha1, tau, sigma, theta, beta,
+                                                gamma))
 
     def TGVext(self, params, start=1, u_init=None):
         it = C.c_int32(0)

@@ -71,6 +71,26 @@ def tvl1_case(name, seed, w, h, niters):
     np.savez_compressed(HERE / f"{name}.npz", ref=fr.ref, depth_in=d0, znear=znear, zfar=zfar, niters=niters, out=out)
 
 
+def tgv_sparse_case(name, seed, w, h, niters, frac, **kw):
+    """PlaneSweep::TGVdenoiseFromSparse: start at a noisy depthmap, pull
+    towards a sparse set of (noisy) samples, the rest of the pixels 0."""
+    fr, _, _ = scenes.config_tiny(seed=seed, width=w, height=h, n_src=1)
+    rng = np.random.default_rng(seed)
+    gt = fr.depth_gt
+    d0 = (gt * (1 + 0.03 * rng.standard_normal(gt.shape))).astype(np.float32)
+    sparse = np.where(rng.random(gt.shape) < frac, gt * (1 + 0.005 * rng.standard_normal(gt.shape)), 0)
+    sparse = sparse.astype(np.float32)
+    zfar = 5.0
+    out = po.ref_tgv_sparse(fr.ref, d0, sparse, zfar, niters, **kw)
+    np.savez_compressed(HERE / f"{name}.npz", ref=fr.ref, depthmap=d0, sparse=sparse, zfar=zfar, niters=niters,
+                        params=np.array([kw.get(k, d) for k, d in SPARSE_DEFAULTS]), out=out)
+
+
+# (name, default) of PlaneSweep::TGVdenoiseFromSparse's numeric arguments, in order
+SPARSE_DEFAULTS = (("alpha0", 2.0), ("alpha1", 1.5), ("tau", 0.02), ("sigma", 1.0), ("theta", 1.0), ("beta", 0.0),
+                   ("gamma", 1.0))
+
+
 def fusion_case(name, seed, dims, bins, n_maps, w, h, iters, interleaved):
     fi = scenes.fusion_sequence(seed, n_maps, w, h)
     vol = po.RefVolume(bins, dims, fi.vol_min, fi.vol_max)
@@ -98,9 +118,14 @@ def fusion_case(name, seed, dims, bins, n_maps, w, h, iters, interleaved):
                         hist=g["hist"])
 
 
-def main():
+def main(only=None):
+    """Regenerate every fixture, or only those whose names are listed."""
     if po.ref_lib() is None:
         raise SystemExit("oracle/_ref/libmvs_ref.so is not built (make -C oracle ref)")
+    if only:
+        for n in only:
+            CASES[n]()
+        return
     sweep_case("sweep_inverse_w5", seed=11, w=64, h=48, n_src=2, n_planes=16, win=5, planes_kind="inverse")
     sweep_case("sweep_refloop_w7", seed=12, w=56, h=40, n_src=3, n_planes=24, win=7, planes_kind="refloop")
     sweep_case("sweep_inverse_w3_negthr", seed=13, w=40, h=36, n_src=2, n_planes=12, win=3, planes_kind="inverse",
@@ -116,9 +141,19 @@ def main():
                 interleaved=False)
     fusion_case("fusion_b10_decoupled", seed=44, dims=(12, 10, 8), bins=10, n_maps=3, w=40, h=32, iters=6,
                 interleaved=False)
+    for c in CASES.values():
+        c()
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
 
+CASES = {
+    "tgv_sparse": lambda: tgv_sparse_case("tgv_sparse", seed=51, w=48, h=40, niters=60, frac=0.1),
+    "tgv_sparse_tensor": lambda: tgv_sparse_case("tgv_sparse_tensor", seed=52, w=37, h=29, niters=45, frac=0.25,
+                                                 alpha0=1.3, alpha1=0.9, tau=0.05, sigma=2.0, theta=0.5, beta=2.5,
+                                                 gamma=0.7),
+}
+
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

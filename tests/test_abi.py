@@ -60,6 +60,12 @@ def test_null_pointer_and_size_errors():
     assert L.mvs_tgv2_run(8, 8, 0, *([None] * 7), 0, 1.0, None, None, None, None, 0, None) == M.MVS_ERR_ARG
     assert L.mvs_ps_run_algorithm(None) == M.MVS_ERR_ARG
     assert L.mvs_tgv2_workspace_bytes(0, 4, 1) == 0
+    assert L.mvs_tgv2_sparse(8, 8, None, None, None, 5.0, 10, *([1.0] * 7), None, None, 0, None) == M.MVS_ERR_ARG
+    assert L.mvs_tgv2_sparse(0, 8, *([None] * 3), 5.0, 10, *([1.0] * 7), *([None] * 2), 0, None) == M.MVS_ERR_ARG
+    assert L.mvs_tgv2_sparse_workspace_bytes(0, 4) == 0
+    # 8 state fields double-buffered + ref, T11, T12, T22, weights, Ds
+    assert L.mvs_tgv2_sparse_workspace_bytes(640, 480) == 640 * 480 * 4 * 22
+    assert L.mvs_ps_tgv_denoise_from_sparse(None, None, 1, *([1.0] * 7)) == M.MVS_ERR_ARG
     assert L.mvs_tvl1_workspace_bytes(640, 480) >= 640 * 480 * 4 * 11
 
 

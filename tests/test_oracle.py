@@ -74,6 +74,25 @@ def test_tvl1_f32_bit_exact_vs_golden(golden):
     np.testing.assert_array_equal(o, g["out"])
 
 
+SPARSE_PARAMS = ("alpha0", "alpha1", "tau", "sigma", "theta", "beta", "gamma")
+
+
+@pytest.mark.parametrize("name", ["tgv_sparse", "tgv_sparse_tensor"])
+def test_tgv_sparse_f32_bit_exact_vs_golden(golden, name):
+    """PlaneSweep::TGVdenoiseFromSparse: the f32 restatement equals the
+    reference's kernels bit for bit (with the reference's v / vbar aliasing);
+    the f64 form stays within 1e-5 relative of them."""
+    g = golden(name)
+    kw = dict(zip(SPARSE_PARAMS, (float(x) for x in g["params"])))
+    args = (g["ref"], g["depthmap"], g["sparse"], float(g["zfar"]), int(g["niters"]))
+    np.testing.assert_array_equal(po.tgv_sparse(*args, precision="f32", **kw), g["out"])
+    o64 = po.tgv_sparse(*args, precision="f64", **kw)
+    assert np.max(np.abs(o64 - g["out"]) / np.abs(g["out"])) < 1e-5
+    # theta reaches only the over-relaxed u, which nothing reads
+    kw["theta"] = 0.1
+    np.testing.assert_array_equal(po.tgv_sparse(*args, precision="f32", **kw), g["out"])
+
+
 @pytest.mark.parametrize("name", ["fusion_b7_decoupled", "fusion_b8_interleaved", "fusion_b2_decoupled",
                                   "fusion_b10_decoupled"])
 def test_fusion_f32_bit_exact_vs_golden(golden, name):
@@ -172,3 +191,9 @@ def test_live_fusion_and_tgv_vs_reference():
     uo, _, _ = po.tgv2(fr.ref, fr.srcs, fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, p, niters=7, warps=2,
                        beta=1.5, gamma=0.8, precision="f32")
     np.testing.assert_array_equal(ur, uo)
+    rng = np.random.default_rng(104)
+    sp = np.where(rng.random(fr.depth_gt.shape) < 0.3, fr.depth_gt, 0).astype(np.float32)
+    d0 = (fr.depth_gt * 1.05).astype(np.float32)
+    sr = po.ref_tgv_sparse(fr.ref, d0, sp, 6.0, 11, beta=1.5, gamma=0.8, theta=0.7)
+    so = po.tgv_sparse(fr.ref, d0, sp, 6.0, 11, beta=1.5, gamma=0.8, precision="f32")
+    np.testing.assert_array_equal(sr, so)
