@@ -255,6 +255,60 @@ def run_reference_gpu(fr, planes, dev, d_ref, d_srcs, wta_depth):
     return out
 
 
+SPARSE_ITERS = 200
+SPARSE_BYTES_PER_PIXEL_ITERATION = 84   # u, v(2), p(2), q(3) read and written + T(3), weight, Ds read; fp32
+
+
+def run_tgv_sparse(fr, dev, d_ref, wta_depth, peak_gbs, reference_gpu):
+    """PlaneSweep::TGVdenoiseFromSparse on the bench frame: TGV2 from the WTA depth towards a
+    seeded 5% sample of the true depth, 200 iterations, one fused launch per iteration; beside
+    it the reference's own three launches per iteration on this GPU."""
+    import torch
+    import mvs_b200 as M
+    rng = np.random.default_rng(77)
+    gt = fr.depth_gt
+    sparse = np.where(rng.random(gt.shape) < 0.05, gt, 0).astype(np.float32)
+    d_sp = torch.from_numpy(sparse).to(dev)
+    out = torch.empty((H, W), device=dev)
+    ws = torch.empty(M.tgv2_sparse_workspace_bytes(W, H) // 8 + 1, dtype=torch.int64, device=dev)
+    times = {}
+    for iters in (0, SPARSE_ITERS):
+        tm = []
+        for k in range(4):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            M.tgv2_sparse(d_ref, wta_depth, d_sp, 8.0, out, ws, iters)
+            b.record()
+            torch.cuda.synchronize()
+            if k:
+                tm.append(a.elapsed_time(b))
+        times[iters] = min(tm)
+    per_it = (times[SPARSE_ITERS] - times[0]) / SPARSE_ITERS
+    res = {"workload": f"640x480, {SPARSE_ITERS} iterations, 5% of the pixels sampled, from the WTA depth",
+           "ms": times[SPARSE_ITERS], "ms_per_iteration": per_it,
+           "roofline": {"bound": "hbm", "achieved": SPARSE_BYTES_PER_PIXEL_ITERATION * W * H / (per_it / 1e3) / 1e9,
+                        "peak": peak_gbs, "unit": "GB/s",
+                        "bytes_per_pixel_iteration": SPARSE_BYTES_PER_PIXEL_ITERATION,
+                        "note": "the 25.8 MB state is L2-resident across iterations"}}
+    res["roofline"]["frac"] = res["roofline"]["achieved"] / peak_gbs
+    if reference_gpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle as po
+        if po.ref_gpu_lib() is not None:
+            u0 = wta_depth.cpu().numpy()
+            rt = []
+            for k in range(2):
+                ru, t = po.ref_gpu_tgv_sparse(fr.ref, u0, sparse, 8.0, SPARSE_ITERS)
+                rt.append(t)
+            mine = out.cpu().numpy()
+            rel = np.abs(mine - ru) / np.maximum(np.abs(ru), 1e-30)
+            res["reference_gpu_ms"] = rt[-1]
+            res["speedup_vs_reference_gpu"] = rt[-1] / times[SPARSE_ITERS]
+            # the reference's GPU build contracts multiply-adds (nvcc default), this engine does not
+            res["max_rel_diff_vs_reference_gpu"] = float(np.nanmax(rel))
+    return res
+
+
 def run_batched(args, dev, stream, flush, rank):
     """the mixed 48-frame batch through mvs_batch (one graph launch per batch)."""
     import time
@@ -351,6 +405,8 @@ def main():
     ap.add_argument("--batch-frames", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fusion", dest="fusion", action="store_false")
+    ap.add_argument("--no-tgv-sparse", dest="tgv_sparse", action="store_false",
+                    help="skip the TGVdenoiseFromSparse timing")
     ap.add_argument("--fusion-dims", type=int, default=256, help="voxels per side of the fusion volume")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -495,6 +551,10 @@ def main():
     ref_gpu = None
     if args.reference_gpu and rank == 0:
         ref_gpu = run_reference_gpu(fr, planes, dev, d_ref, d_srcs, wta_depth if tgv_ms else None)
+
+    tgv_sparse = None
+    if args.tgv_sparse and rank == 0:
+        tgv_sparse = run_tgv_sparse(fr, dev, d_ref, wta_depth, peaks()[0], args.reference_gpu)
 
     # --- batched uneven frames: 48 frames (320x240 / 640x480 rooms, 1242x375 street)
     #     with 64-256 planes, 4-8 views and 5x5-11x11 windows in one graph launch; the autotuner
@@ -654,6 +714,7 @@ def main():
         "fusion": fusion,
         "batched": batched,
         "reference_gpu": ref_gpu,
+        "tgv_sparse": tgv_sparse,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clock_summary,
     }

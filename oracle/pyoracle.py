@@ -234,8 +234,24 @@ def ref_gpu_lib():
         L.ref_gpu_tgv.restype = C.c_double
         L.ref_gpu_tgv.argtypes = ([C.c_int, C.c_int, P, P, C.c_int, P, P, P, P, P, C.c_int, C.c_int, C.c_int] +
                                   [C.c_double] * 7 + [P, P])
+        L.ref_gpu_tgv_sparse.restype = C.c_double
+        L.ref_gpu_tgv_sparse.argtypes = [C.c_int, C.c_int, P, P, P, C.c_float, C.c_int] + [C.c_double] * 7 + [P]
         _ref_gpu = L
     return _ref_gpu
+
+
+def ref_gpu_tgv_sparse(ref, depthmap, sparse, zfar, niters, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, theta=1.0,
+                       beta=0.0, gamma=1.0):
+    """PlaneSweep::TGVdenoiseFromSparse's call sequence with the reference's
+    own kernels on the GPU; returns (u, device ms)."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref/libmvs_ref_gpu.so not built")
+    h, w = ref.shape
+    out = np.zeros((h, w), np.float32)
+    ms = L.ref_gpu_tgv_sparse(w, h, _fp(_f32(ref)), _fp(_f32(depthmap)), _fp(_f32(sparse)), float(zfar), niters,
+                              alpha0, alpha1, tau, sigma, theta, beta, gamma, _fp(out))
+    return out, ms
 
 
 def ref_gpu_sweep(ref, srcs, K_1based, Rref, tref, src_poses, planes, winsize, zfar, stdthresh=1e-4,

@@ -4,8 +4,8 @@
  * kernels.cu and TGV2_kernels.cu, compiled unchanged for sm_100a where they
  * lie in the reference tree (oracle/Makefile, target ref_gpu).  The functions
  * replay the call sequences of PlaneSweep::RunAlgorithm / PlaneSweepThread
- * (planesweep.cpp:74-259) and PlaneSweep::TGV (planesweep.cpp:381-536) on
- * device images, exactly as ref_driver.cpp replays them on host images for
+ * (planesweep.cpp:74-259), PlaneSweep::TGV (planesweep.cpp:381-536) and
+ * PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674) on device images, exactly as ref_driver.cpp replays them on host images for
  * the CPU build: the reference's wrappers, kernels and Matrix3D arithmetic,
  * one launch per wrapper call.  Buffers are allocated before the timed
  * region; buffers the reference leaves uninitialised are zero-filled.
@@ -213,6 +213,54 @@ double ref_gpu_tgv(int w, int h, const float *refimg, const float *srcs, int nsr
         delete Iu[i];
         delete r[i];
     }
+    if (cudaGetLastError() != cudaSuccess) return -1.0;
+    return ms;
+}
+
+/* PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674) on the GPU:
+ * weights, scaled sparse and start depth, the tensor, then niters x (P on u,
+ * Q, the sparse tensor U step with vxbar / vybar passed as both v and its
+ * over-relaxation), u * zfar.  Returns the device time (ms) from the first
+ * kernel to the last, or a negative value on a CUDA error. */
+double ref_gpu_tgv_sparse(int w, int h, const float *refimg, const float *depthmap, const float *sparse, float zfar,
+                          int niters, double alpha0, double alpha1, double tau, double sigma, double theta,
+                          double beta, double gamma, float *out)
+{
+    const size_t n = (size_t)w * h;
+    Grid g(w, h);
+    const dim3 &B = g.blocks, &T = g.threads;
+    Dev px(n), py(n), qx(n), qy(n), qz(n), qw(n), ubar(n), vxbar(n), vybar(n), weights(n), Ds(n), ref(n), T1(n),
+        T2(n), T3(n), T4(n), u(n);
+    cudaMemcpy(Ds.p, sparse, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(ubar.p, depthmap, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(ref.p, refimg, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaEvent_t ea, eb;
+    cudaEventCreate(&ea);
+    cudaEventCreate(&eb);
+    cudaDeviceSynchronize();
+    cudaEventRecord(ea);
+    calculateWeights_sparseDepth(weights.p, Ds.p, w, h, B, T);
+    element_scale(Ds.p, 1.f / zfar, w, h, B, T);
+    element_scale(ubar.p, 1.f / zfar, w, h, B, T);
+    cudaMemcpy(u.p, ubar.p, n * sizeof(float), cudaMemcpyDeviceToDevice);
+    element_scale(ref.p, 1.f / 255.f, w, h, B, T);
+    Anisotropic_diffusion_tensor(T1.p, T2.p, T3.p, T4.p, ref.p, beta, gamma, w, h, B, T);
+    for (int i = 0; i < niters; ++i) {
+        TGV2_updateP_tensor_weighed(px.p, py.p, T1.p, T2.p, T3.p, T4.p, u.p, vxbar.p, vybar.p, alpha1, sigma, w, h, B,
+                                    T);
+        TGV2_updateQ(qx.p, qy.p, qz.p, qw.p, vxbar.p, vybar.p, alpha0, sigma, w, h, B, T);
+        TGV2_updateU_sparseDepthTensor(u.p, vxbar.p, vybar.p, ubar.p, vxbar.p, vybar.p, T1.p, T2.p, T3.p, T4.p, px.p,
+                                       py.p, qx.p, qy.p, qz.p, qw.p, weights.p, Ds.p, alpha0, alpha1, tau, theta, w, h,
+                                       B, T);
+    }
+    element_scale(u.p, zfar, w, h, B, T);
+    cudaEventRecord(eb);
+    cudaEventSynchronize(eb);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ea, eb);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+    cudaMemcpy(out, u.p, n * sizeof(float), cudaMemcpyDeviceToHost);
     if (cudaGetLastError() != cudaSuccess) return -1.0;
     return ms;
 }

@@ -407,8 +407,11 @@ struct __align__(16) AggSmem {
     Smem S;
     float Rf[TH + 16][RWMAX];   // reference region (shifted in the compensated mode)
     float Yc[TH + 16];          // region row coordinates (1-based, mirrored)
-    float RM[TH][RWMAX];        // reference window sums / means per output pixel
-    float RS[TH][RWMAX];        // reference n^2 var / std per output pixel
+    // reference window sums / means and n^2 var / std per output pixel; rows
+    // at the CSP pitch, so the four rows one warp reads in pass B sit on
+    // distinct banks (at a 64-float pitch they were a 4-way conflict)
+    float RM[TH][CSP];
+    float RS[TH][CSP];
 };
 
 // Each source pixel's 2x2 bilinear neighbourhood (x, x+1 on rows y, y+1) as

@@ -108,3 +108,19 @@ def test_planesweep_handle_tgv_denoise_from_sparse(cuda, golden):
     np.testing.assert_array_equal(got, want)
     with pytest.raises(ValueError):
         ps.TGVdenoiseFromSparse(sparse[:-1], 10)
+
+
+def test_sparse_vs_the_reference_gpu_build(cuda):
+    """Against the reference's own kernels compiled for this GPU (its nvcc build
+    contracts multiply-adds, so agreement is to rounding, not bits), with two
+    theta values: the over-relaxation the reference computes is not read, in
+    its GPU build as in its CPU build."""
+    if po.ref_gpu_lib() is None:
+        pytest.skip("oracle/_ref/libmvs_ref_gpu.so not built")
+    ref, depth, sparse = sparse_case(11, 97, 61, frac=0.2)
+    out = run_sparse(cuda, ref, depth, sparse, 6.0, 40)
+    for theta in (1.0, 0.3):
+        ru, ms = po.ref_gpu_tgv_sparse(ref, depth, sparse, 6.0, 40, theta=theta)
+        assert ms >= 0
+        rel = np.abs(out - ru) / np.abs(ru)
+        assert rel.max() <= 1e-5, (theta, rel.max())
