@@ -105,7 +105,9 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
     if (rx >= G::RW) return;
     // X-dependent part of the homography, once per plane
     const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
-    const float wm1 = (float)(w - 1), hm1 = (float)(h - 1);
+    // fx + 1 <= w - 1 is fx <= w - 2 for the integer-valued fx (also for
+    // |fx| >= 2^24, inf and NaN, where both forms agree)
+    const float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
 #pragma unroll
     for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
         float fa[BATCH], fb[BATCH];
@@ -136,7 +138,7 @@ __device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restr
                 }
                 const float fx = floorf(xs), fy = floorf(ys);
                 // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
-                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= wm1 && fy + 1.f <= hm1;
+                ok[j] = fx >= 0.f && fy >= 0.f && fx <= wm2 && fy <= hm2;
                 if (ok[j]) {
                     const int xi = (int)fx, yi = (int)fy;
                     fa[j] = xs - fx;
@@ -446,7 +448,9 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
     const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
     if (rx >= G::RW) return;
     const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
-    const float wm1 = (float)(w - 1), hm1 = (float)(h - 1);
+    // fx + 1 <= w - 1 is fx <= w - 2 for the integer-valued fx (also for
+    // |fx| >= 2^24, inf and NaN, where both forms agree)
+    const float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
 #pragma unroll
     for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
         float fa[BATCH], fb[BATCH];
@@ -475,7 +479,7 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
                     ys = fmaf(q1, rz, -1.f);
                 }
                 const float fx = floorf(xs), fy = floorf(ys);
-                ok[j] = fx >= 0.f && fy >= 0.f && fx + 1.f <= wm1 && fy + 1.f <= hm1;
+                ok[j] = fx >= 0.f && fy >= 0.f && fx <= wm2 && fy <= hm2;
                 if (ok[j]) {
                     fa[j] = xs - fx;
                     fb[j] = ys - fy;
