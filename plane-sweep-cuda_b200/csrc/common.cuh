@@ -54,6 +54,34 @@ __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// Programmatic dependent launch, for loops of short dependent launches (one
+// launch per iteration).  A kernel launched with launch_dependent() may be
+// scheduled while the previous kernel of its stream is still finishing, which
+// hides the gap between the two launches (about 2.6 us per launch measured on
+// the B200).  Such a kernel calls wait_for_previous_grid() before it reads or
+// writes any global memory that the previous kernels of the stream touch: the
+// wait returns once those grids have completed and their writes are visible.
+// Without the launch attribute the wait returns at once.
+__device__ __forceinline__ void wait_for_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                             Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, ((KArgs)args)...);
+}
+
 // One frame of a batched sweep (device copy; see sweep_batch_kernel).
 struct BatchFrameDev {
     const float *ref, *srcs, *H, *depths;

@@ -187,6 +187,8 @@ __global__ void __launch_bounds__(VX *VY) update_u_kernel(Dims D, const uint16_t
                                                          float *__restrict__ u, float *__restrict__ v,
                                                          const float *__restrict__ p, double tau, double lambda)
 {
+    wait_for_previous_grid();   // launched as a dependent launch: the previous step is complete
+    allow_next_grid();
     constexpr int HS = HistStride<BINS>::value;
     const int x = blockIdx.x * VX + threadIdx.x, y = blockIdx.y * VY + threadIdx.y, z = blockIdx.z;
     if (x >= D.vw || y >= D.vh) return;
@@ -211,6 +213,8 @@ __global__ void __launch_bounds__(VX *VY) update_u_kernel(Dims D, const uint16_t
 __global__ void __launch_bounds__(VX *VY) update_p_kernel(Dims D, const float *__restrict__ v, float *__restrict__ p,
                                                          float sigma)
 {
+    wait_for_previous_grid();   // launched as a dependent launch: the previous step is complete
+    allow_next_grid();
     const int x = blockIdx.x * VX + threadIdx.x, y = blockIdx.y * VY + threadIdx.y, z = blockIdx.z;
     if (x >= D.vw || y >= D.vh) return;
     const size_t sz = (size_t)D.vw * D.vh, n = sz * D.vd;
@@ -329,7 +333,7 @@ int fusion_update_u(int vw, int vh, int vd, int bins, const uint16_t *hist, floa
 {
     const Dims D = dims_of(vw, vh, vd, kZero3, kZero3);
     switch (bins) {
-#define U(N) case N: update_u_kernel<N><<<voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st>>>(D, hist, u, v, p, tau, lambda); break;
+#define U(N) case N: MVS_TRY_CUDA(launch_dependent(update_u_kernel<N>, voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st, D, hist, u, v, p, tau, lambda)); break;
         MVS_BINS(U)
 #undef U
     default: return set_error(MVS_ERR_ARG, "bins %d not supported (2..10)", bins);
@@ -340,7 +344,7 @@ int fusion_update_u(int vw, int vh, int vd, int bins, const uint16_t *hist, floa
 int fusion_update_p(int vw, int vh, int vd, const float *v, float *p, double sigma, cudaStream_t st)
 {
     const Dims D = dims_of(vw, vh, vd, kZero3, kZero3);
-    update_p_kernel<<<voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st>>>(D, v, p, (float)sigma);
+    MVS_TRY_CUDA(launch_dependent(update_p_kernel, voxel_grid(vw, vh, vd), dim3(VX, VY), 0, st, D, v, p, (float)sigma));
     return check_launch("fusion update_p_kernel");
 }
 

@@ -239,6 +239,8 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     __shared__ float sU[TY + 2][TX + 2], sVX[TY + 2][TX + 2], sVY[TY + 2][TX + 2];
     __shared__ float sPx[TY + 1][TX + 1], sPy[TY + 1][TX + 1];
     __shared__ float sQx[TY + 1][TX + 1], sQy[TY + 1][TX + 1], sQz[TY + 1][TX + 1];
+    wait_for_previous_grid();   // launched as a dependent launch: the previous iteration is complete
+    allow_next_grid();
     const int w = b.w, h = b.h;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
@@ -964,10 +966,9 @@ struct SparseBufs {
 
 // Tile of SX x SY pixels per CTA of SNT threads, two rows per thread in the
 // primal step (the p, q halo is then 6% of the tile instead of 16%).  The
-// launch is bound by the dependent chains of the reference's double-precision
-// projections (square root and divisions, kept for bit parity); neither one
-// wave of CTAs nor loading every operand ahead of the first barrier changed
-// its time.
+// iterations are dependent launches (launch_dependent): each waits for the
+// previous one before its first global access, and its launch overlaps the
+// previous one's tail.
 constexpr int SX = 32, SY = 16, SNT = 256;
 
 __global__ void __launch_bounds__(SNT) sparse_iteration_kernel(SparseBufs b)
@@ -978,6 +979,8 @@ __global__ void __launch_bounds__(SNT) sparse_iteration_kernel(SparseBufs b)
     const int w = b.w, h = b.h;
     const int x0 = blockIdx.x * SX, y0 = blockIdx.y * SY;
     const int tid = threadIdx.x;
+    wait_for_previous_grid();   // the previous iteration's state (or the set-up) is complete
+    allow_next_grid();          // the next iteration may be scheduled; it waits the same way
     for (int k = tid; k < (SX + 2) * (SY + 2); k += SNT) {
         const int ry = k / (SX + 2), rx = k % (SX + 2);
         const int px = min(max(x0 - 1 + rx, 0), w - 1), py = min(max(y0 - 1 + ry, 0), h - 1);
@@ -1159,7 +1162,7 @@ int tgv2_sparse_run(int w, int h, const float *ref255, const float *depthmap, co
         b.Qx_out = L.Qx[cur ^ 1];
         b.Qy_out = L.Qy[cur ^ 1];
         b.Qz_out = L.Qz[cur ^ 1];
-        sparse_iteration_kernel<<<gi, bi, 0, st>>>(b);
+        MVS_TRY_CUDA(launch_dependent(sparse_iteration_kernel, gi, bi, 0, st, b));
         cur ^= 1;
     }
     scale_kernel<<<eg, 256, 0, st>>>(L.u[cur], n, zfar, out);
@@ -1359,10 +1362,11 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             ib.Qx_out = L.Qx[cur ^ 1];
             ib.Qy_out = L.Qy[cur ^ 1];
             ib.Qz_out = L.Qz[cur ^ 1];
-            if (V <= 4) iteration_kernel<4><<<gi, bi, 0, st>>>(ib);
-            else if (V <= 8) iteration_kernel<8><<<gi, bi, 0, st>>>(ib);
-            else if (V <= 16) iteration_kernel<16><<<gi, bi, 0, st>>>(ib);
-            else iteration_kernel<32><<<gi, bi, 0, st>>>(ib);
+            // dependent launches: each iteration's launch overlaps the previous one's tail
+            if (V <= 4) MVS_TRY_CUDA(launch_dependent(iteration_kernel<4>, gi, bi, 0, st, ib));
+            else if (V <= 8) MVS_TRY_CUDA(launch_dependent(iteration_kernel<8>, gi, bi, 0, st, ib));
+            else if (V <= 16) MVS_TRY_CUDA(launch_dependent(iteration_kernel<16>, gi, bi, 0, st, ib));
+            else MVS_TRY_CUDA(launch_dependent(iteration_kernel<32>, gi, bi, 0, st, ib));
             cur ^= 1;
             ++total;
             if (prm->tol > 0 && (k + 1) % check_every == 0) {

@@ -67,6 +67,8 @@ __global__ void __launch_bounds__(TX *TY) tvl1_iteration_kernel(Bufs b)
 {
     __shared__ float sD[TY + 2][TX + 2];
     __shared__ float sPx[TY + 1][TX + 1], sPy[TY + 1][TX + 1];
+    wait_for_previous_grid();   // launched as a dependent launch: the previous iteration is complete
+    allow_next_grid();
     const int w = b.w, h = b.h;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
@@ -191,7 +193,7 @@ int tvl1_run(int w, int h, const float *ref255, float *depth, float znear, float
         b.out = L.D[cur ^ 1];
         b.Px_out = L.Px[cur ^ 1];
         b.Py_out = L.Py[cur ^ 1];
-        tvl1_iteration_kernel<<<g2, b2, 0, st>>>(b);
+        MVS_TRY_CUDA(launch_dependent(tvl1_iteration_kernel, g2, b2, 0, st, b));
         cur ^= 1;
     }
     tvl1_finish_kernel<<<min(ceil_div(n, 256), 8 * kSMs), 256, 0, st>>>(L.D[cur], n, zfar - znear, znear, depth);
