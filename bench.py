@@ -41,10 +41,12 @@ UNIT = "Mpix*planes/s"
 # per-launch DRAM traffic (bytes) of the dominant kernels, from one `ncu --set full` capture each
 # of `python bench.py --steps 2 --warmup 3 --tgv-steps 1 --no-cpu-baseline --no-batch
 # --no-warm-start --no-fusion --no-reference-gpu` (one launch, dram__bytes_read.sum +
-# dram__bytes_write.sum); the persistent TGV2 launch covers 500 iterations
+# dram__bytes_write.sum; the TGV2 iteration also with --no-tgv-sparse, launch 51: ncu runs every
+# launch with a cold L2, so that figure is the whole working set, which stays in L2 between the
+# back-to-back iterations of a run)
 NCU_TRAFFIC = {"sweep_aggregated_kernel": 45.78944e6 + 116.774656e6,
                "wta_volume_kernel": 157.294336e6 + 3.661312e6,
-               "tgv2_iteration_kernel": (62.196992e6 + 3.11296e6) / 500}
+               "tgv2_iteration_kernel": 47.945216e6 + 0.405248e6}
 # algorithmic FP32 operations per (pixel, plane, view) evaluation of the fused sweep: homography
 # 15 (kernels.cu:31-44), bilinear 8 (kernels.cu:4-29), three running window moments 14
 # (kernels.cu:187-235), NCC 10 (kernels.cu:46-64), running best 3 (kernels.cu:66-82)
@@ -664,7 +666,7 @@ def main():
     if tgv_ms:
         it_ms = tgv_ms_frame / max(tgv_iters, 1)
         tb = (8 * (8 + V) + 4 * (4 + 2 * V)) * W * H
-        tgv_roofline = {"bound": "hbm", "kernel": "tgv2_persistent_kernel (state on chip)",
+        tgv_roofline = {"bound": "hbm", "kernel": "iteration_kernel<8> (one dependent launch per iteration)",
                         "achieved": tb / (it_ms / 1e3) / 1e9,
                         "peak": hbm, "unit": "GB/s", "frac": tb / (it_ms / 1e3) / 1e9 / hbm,
                         "bytes_per_iteration": tb, "ms_per_iteration_incl_energy_checks": it_ms,

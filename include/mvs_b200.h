@@ -156,9 +156,11 @@ typedef struct mvs_tgv2_params {
     int32_t iteration_kernel; /* MVS_TGV2_ITER_*: how the iterations run (same results) */
 } mvs_tgv2_params;
 
-#define MVS_TGV2_ITER_AUTO 0     /* one cooperative launch per linearisation with the state on
-                                    chip when the image fits one tile per SM, else as below */
-#define MVS_TGV2_ITER_LAUNCH 1   /* one fused launch per iteration, state in HBM/L2 */
+#define MVS_TGV2_ITER_AUTO 0     /* the fastest measured form: as MVS_TGV2_ITER_LAUNCH */
+#define MVS_TGV2_ITER_LAUNCH 1   /* one fused launch per iteration (dependent launches, state in
+                                    L2), energy checks and the stopping test on the device */
+#define MVS_TGV2_ITER_PERSISTENT 2 /* one cooperative launch per linearisation with the state on
+                                    chip, when the image fits one tile per SM (else as LAUNCH) */
 
 size_t mvs_tgv2_workspace_bytes(int32_t width, int32_t height, int32_t n_views);
 

@@ -273,7 +273,7 @@ def sweep_wta_volume(cost, depths, n_pixels, n_planes, zfar, depth_out, labels=N
 # TGV2 / TV-L1 (device tensors)
 # ---------------------------------------------------------------------------
 
-TGV2_ITER_AUTO, TGV2_ITER_LAUNCH = 0, 1
+TGV2_ITER_AUTO, TGV2_ITER_LAUNCH, TGV2_ITER_PERSISTENT = 0, 1, 2
 
 
 def tgv2_params(niters=30, warps=15, lam=0.5, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0,
