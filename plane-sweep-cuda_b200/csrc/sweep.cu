@@ -74,171 +74,15 @@ struct SweepArgs {
 
 // Thread t always owns region column rx = t & 63 and rows (t >> 6) + 4k, so its
 // pixel column X and its CELLS pixel rows Y_k (mirrored at the image border)
-// are fixed for the whole CTA: `Ycol` holds them, and per plane only the
-// X-dependent part of H*(X, Y, 1) is formed once (COMPENSATED; the REFERENCE
-// path keeps the reference's dot-product order).  Cells are processed in
+// are fixed for the whole CTA: the rows sit in shared memory (Yc), and per
+// plane only the X-dependent part of H*(X, Y, 1) is formed once (COMPENSATED;
+// the REFERENCE path keeps the reference's dot-product order).  Cells are processed in
 // batches -- coordinates, then all gathers, then the interpolation -- so each
 // thread keeps several independent L1/L2 gathers in flight.
 template <int WIN>
 struct A0Cells {
     static constexpr int CELLS = (Geo<WIN>::RH * RWMAX + THREADS - 1) / THREADS;
 };
-
-template <int WIN>
-__device__ __forceinline__ void a0_setup(int w, int h, int x0, int y0, float &Xcol, float *Ycol)
-{
-    using G = Geo<WIN>;
-    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
-    Xcol = (float)(mirror_idx(x0 - G::R + rx, w) + 1);
-#pragma unroll
-    for (int k = 0; k < A0Cells<WIN>::CELLS; ++k) Ycol[k] = (float)(mirror_idx(y0 - G::R + rb + 4 * k, h) + 1);
-}
-
-template <int WIN, int MOM>
-__device__ __forceinline__ void pass_a0(float (*Wt)[RWMAX], const float *__restrict__ src, int w, int h,
-                                        const float *Hm, float X, const float *Ycol)
-{
-    using G = Geo<WIN>;
-    constexpr int CELLS = A0Cells<WIN>::CELLS;
-    constexpr int BATCH = 4;
-    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
-    if (rx >= G::RW) return;
-    // X-dependent part of the homography, once per plane
-    const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
-    // fx + 1 <= w - 1 is fx <= w - 2 for the integer-valued fx (also for
-    // |fx| >= 2^24, inf and NaN, where both forms agree)
-    const float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
-#pragma unroll
-    for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
-        float fa[BATCH], fb[BATCH];
-        int off[BATCH];
-        bool ok[BATCH];
-#pragma unroll
-        for (int j = 0; j < BATCH; ++j) {
-            const int k = k0 + j;
-            ok[j] = false;
-            off[j] = 0;
-            fa[j] = fb[j] = 0.f;
-            if (k < CELLS && rb + 4 * k < G::RH) {
-                const float Y = Ycol[k];
-                float xs, ys;
-                if (MOM == MVS_MOMENTS_REFERENCE) {
-                    // h * (l+1, k+1, 1), then x / x.z - 1 (kernels.cu:39-40), no contraction
-                    const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
-                    const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
-                    const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
-                    xs = q0 / q2 - 1.f;
-                    ys = q1 / q2 - 1.f;
-                } else {
-                    const float q0 = fmaf(Hm[1], Y, a0), q1 = fmaf(Hm[4], Y, a1), q2 = fmaf(Hm[7], Y, a2);
-                    float rz;
-                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rz) : "f"(q2));
-                    xs = fmaf(q0, rz, -1.f);
-                    ys = fmaf(q1, rz, -1.f);
-                }
-                const float fx = floorf(xs), fy = floorf(ys);
-                // outside [0, W-2] x [0, H-2] (or non-finite) reads as 0 (kernels.cu:21)
-                ok[j] = fx >= 0.f && fy >= 0.f && fx <= wm2 && fy <= hm2;
-                if (ok[j]) {
-                    const int xi = (int)fx, yi = (int)fy;
-                    fa[j] = xs - fx;
-                    fb[j] = ys - fy;
-                    off[j] = yi * w + xi;
-                }
-            }
-        }
-        float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
-#pragma unroll
-        for (int j = 0; j < BATCH; ++j) {
-            d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
-            if (ok[j]) {
-                const float *r0 = src + off[j];
-                d00[j] = ldg(r0);
-                d01[j] = ldg(r0 + 1);
-                d10[j] = ldg(r0 + w);
-                d11[j] = ldg(r0 + w + 1);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < BATCH; ++j) {
-            const int k = k0 + j;
-            if (k >= CELLS || rb + 4 * k >= G::RH) continue;
-            float v = 0.f;
-            if (ok[j]) {
-                const float a = fa[j], b = fb[j];
-                if (MOM == MVS_MOMENTS_REFERENCE) {
-                    const float t1 = a * d01[j] + (1 - a) * d00[j];
-                    const float t2 = a * d11[j] + (1 - a) * d10[j];
-                    v = b * t2 + (1 - b) * t1;
-                } else {
-                    const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
-                    const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
-                    v = fmaf(b, t2 - t1, t1);
-                }
-            }
-            Wt[rb + 4 * k][rx] = v;
-        }
-    }
-}
-
-// ---- pass A1: column sums --------------------------------------------------------
-// thread -> (column c = t & 63, strip s = t >> 6 of 8 output rows); refcol holds
-// the strip's reference values (shifted by `shift` in the compensated mode).
-
-template <int WIN, int MOM>
-__device__ __forceinline__ void pass_a1(float (*Wt)[RWMAX], float (*CS)[TH][CSP], const float *refcol, float shift)
-{
-    using G = Geo<WIN>;
-    const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
-    if (c >= G::RW) return;
-    float wv[G::SROWS];
-#pragma unroll
-    for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[8 * s + i][c];
-    if (MOM == MVS_MOMENTS_REFERENCE) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float s1 = 0.f, s2 = 0.f, s12 = 0.f;
-            // windowed_mean_column_kernel on warped, warped^2 and ref*warped
-#pragma unroll
-            for (int i = 0; i < WIN; ++i) {
-                const float x = wv[k + i];
-                s1 = s1 + x;
-                s2 = s2 + x * x;
-                s12 = s12 + refcol[k + i] * x;
-            }
-            s1 = s1 / (float)WIN;
-            s2 = s2 / (float)WIN;
-            s12 = s12 / (float)WIN;
-            CS[0][8 * s + k][c] = s1;
-            CS[1][8 * s + k][c] = s2;
-            CS[2][8 * s + k][c] = s12;
-        }
-    }
-    if (MOM != MVS_MOMENTS_REFERENCE) {
-        // sliding sums down the strip of shifted values
-#pragma unroll
-        for (int i = 0; i < G::SROWS; ++i) wv[i] -= shift;
-        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
-#pragma unroll
-        for (int i = 0; i < WIN; ++i) {
-            s1 += wv[i];
-            s2 = fmaf(wv[i], wv[i], s2);
-            s12 = fmaf(refcol[i], wv[i], s12);
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k > 0) {
-                const float xn = wv[k + WIN - 1], xo = wv[k - 1];
-                s1 = (s1 + xn) - xo;
-                s2 = fmaf(-xo, xo, fmaf(xn, xn, s2));
-                s12 = fmaf(-refcol[k - 1], xo, fmaf(refcol[k + WIN - 1], xn, s12));
-            }
-            CS[0][8 * s + k][c] = s1;
-            CS[1][8 * s + k][c] = s2;
-            CS[2][8 * s + k][c] = s12;
-        }
-    }
-}
 
 // ---- pass B: row sums of the three column-sum arrays ------------------------------
 // thread -> (row y = t >> 3, segment g = t & 7 of RUN outputs)
