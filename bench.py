@@ -545,6 +545,8 @@ def main():
                 "median_abs_depth_err_m": {"plain": statistics.mean(r["plain_err"] for r in rows),
                                            "warm": statistics.mean(r["warm_err"] for r in rows)},
                 "dual_start": {"sigma_pq": WS.WARM_DUAL_SIGMA, "sigma_r": WS.WARM_DUAL_SIGMA_R},
+                "steps": {"warm": {"tau": WS.WARM_TAU, "sigma": WS.WARM_SIGMA},
+                          "plain": {"tau": 0.02, "sigma": 1.0}},
                 "network": {"weights": WS.WEIGHTS.name, "trained": wmeta},
                 "includes": "network forward + TGV2 to tolerance; scenes rendered on the device, seeds held out"}
 
