@@ -446,7 +446,9 @@ def main():
         M.sweep(desc, d_ref, d_srcs, d_H, d_depths, depth, None, None, cost, wsp)
         M.sweep_wta_volume(cost, d_depths, W * H, P, 8.0, depth, labels, best)
 
-    launches_per_step = 4   # homography, sweep, sweep epilogue, WTA over the volume
+    # homography_kernel, quad_kernel (the sources' 2x2 neighbourhoods), sweep_aggregated_kernel,
+    # wta_finish_kernel (the sweep's epilogue), wta_volume_kernel (WTA over the stored volume)
+    launches_per_step = 5
 
     # clocks and throttle reasons, sampled every 20 ms from before the warm-up to the end
     clocks = ClockSampler(local).__enter__()
