@@ -197,7 +197,7 @@ struct IterCtl {
     int have_energy;   // last_e holds an energy
     int stop_total;    // iteration count at which the tolerance was met
     int energy_at;     // iteration count at which last_e was evaluated
-    int pad;
+    unsigned int blocks_done;   // energy_kernel blocks finished (the last one resets it)
     double prev, last_e;
 };
 
@@ -383,18 +383,27 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
 // reference has none): per-block FP64 partial sums, then one block adds them.
 constexpr int EB = 256;
 
+// The TGV2 energy (no reference symbol: the reference runs a fixed count) of
+// the current state: alpha1 |T (grad u - v)|_2 + alpha0 |eps(v)| + lambda
+// sum_i |It_i + (u - u0) Iu_i| per pixel, in double, with the operators of the
+// P, Q and R updates.  Each block adds its pixels' terms; the block that
+// finishes last (a completion counter, nothing waits) adds the blocks' partial
+// sums in block order, writes the energy and, given `ctl`, applies the
+// stopping test of the launch path: |E_prev - E| <= tol |E_prev| between two
+// checks of one linearisation.  Launches after a met tolerance return at once.
 __global__ void __launch_bounds__(EB) energy_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
                                                     const float *__restrict__ T22, const float *__restrict__ It,
                                                     const float *__restrict__ Iu, const float *__restrict__ u0,
                                                     const float *__restrict__ u, const float *__restrict__ u1x,
                                                     const float *__restrict__ u1y, int w, int h, int V, double lambda,
                                                     double alpha0, double alpha1, double *__restrict__ partial,
-                                                    const IterCtl *ctl)
+                                                    double *__restrict__ out, IterCtl *ctl, double tol, int total)
 {
     __shared__ double red[EB / 32];
+    __shared__ int last;
     wait_for_previous_grid();   // also launched as a dependent launch after the iterations
     allow_next_grid();
-    if (ctl && ctl->done) return;
+    if (ctl->done) return;
     const int n = w * h;
     double e = 0.0;
     for (int i = blockIdx.x * EB + threadIdx.x; i < n; i += gridDim.x * EB) {
@@ -419,52 +428,36 @@ __global__ void __launch_bounds__(EB) energy_kernel(const float *__restrict__ T1
         double s = 0.0;
         for (int k = 0; k < EB / 32; ++k) s += red[k];
         partial[blockIdx.x] = s;
+        __threadfence();   // the partial is visible before the block counts as done
+        last = atomicAdd(&ctl->blocks_done, 1u) == gridDim.x - 1;
     }
-}
-
-// sum_partials_kernel's sum, then the stopping test of the launch path:
-// |E_prev - E| <= tol |E_prev| between two checks of one linearisation.
-__global__ void energy_check_kernel(const double *__restrict__ partial, int m, double *__restrict__ out,
-                                    IterCtl *ctl, double tol, int total)
-{
-    __shared__ double red[EB / 32];
-    wait_for_previous_grid();
-    allow_next_grid();
-    if (ctl->done) return;
-    double s = 0.0;
-    for (int k = threadIdx.x; k < m; k += EB) s += partial[k];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (!last) return;
+    // the last block: every partial is written (each was fenced before its count)
+    __threadfence();
+    double t = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += EB) t += __ldcg(partial + k);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int k = 0; k < EB / 32; ++k) t += red[k];
-        *out = t;
-        if (ctl->have_prev && fabs(ctl->prev - t) <= tol * fabs(ctl->prev)) {
-            ctl->done = 1;
-            ctl->stop_total = total;
-        } else {
-            ctl->prev = t;
-            ctl->have_prev = 1;
+        double E = 0.0;
+        for (int k = 0; k < EB / 32; ++k) E += red[k];
+        *out = E;
+        if (tol > 0) {
+            if (ctl->have_prev && fabs(ctl->prev - E) <= tol * fabs(ctl->prev)) {
+                ctl->done = 1;
+                ctl->stop_total = total;
+            } else {
+                ctl->prev = E;
+                ctl->have_prev = 1;
+            }
+            ctl->last_e = E;
+            ctl->have_energy = 1;
+            ctl->energy_at = total;
         }
-        ctl->last_e = t;
-        ctl->have_energy = 1;
-        ctl->energy_at = total;
-    }
-}
-
-__global__ void sum_partials_kernel(const double *__restrict__ partial, int m, double *__restrict__ out)
-{
-    __shared__ double red[EB / 32];
-    double s = 0.0;
-    for (int k = threadIdx.x; k < m; k += EB) s += partial[k];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int k = 0; k < EB / 32; ++k) t += red[k];
-        *out = t;
+        ctl->blocks_done = 0;   // ready for the next evaluation
     }
 }
 
@@ -516,7 +509,10 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
     }
 }
 
-constexpr int kEnergyBlocks = 2 * kSMs;
+// energy_kernel blocks: one pixel per thread, up to this many blocks (then each
+// thread takes several pixels)
+constexpr int kEnergyBlocksMax = 4096;
+inline int energy_blocks(int n) { return n / EB + 1 < kEnergyBlocksMax ? n / EB + 1 : kEnergyBlocksMax; }
 
 // ---- persistent iteration: the state stays on chip -----------------------------------
 //
@@ -968,7 +964,7 @@ Layout layout(void *base, int w, int h, int V)
     L.It = take(n * V);
     L.Iu = take(n * V);
     L.r = take(n * V);
-    L.partial = (double *)take(2 * kEnergyBlocks);
+    L.partial = (double *)take(2 * kEnergyBlocksMax);
     L.energy = (double *)take(2);
     L.ctl = (IterCtl *)take(sizeof(IterCtl) / sizeof(float));
     for (int k = 0; k < 2; ++k) {
@@ -1318,7 +1314,8 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         MVS_TRY_CUDA(cudaStreamSynchronize(st));
         return MVS_OK;
     };
-    if (!pth && prm->tol > 0) MVS_TRY_CUDA(cudaMemsetAsync(L.ctl, 0, sizeof(IterCtl), st));
+    // (also clears energy_kernel's completion counter, which every run's final energy uses)
+    MVS_TRY_CUDA(cudaMemsetAsync(L.ctl, 0, sizeof(IterCtl), st));
     for (int l = 0; l < prm->warps && !done; ++l) {
         if (!pth && prm->tol > 0 && l > 0)   // a new linearisation has no previous energy
             MVS_TRY_CUDA(cudaMemsetAsync(&L.ctl->have_prev, 0, sizeof(int), st));
@@ -1436,11 +1433,10 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             cur ^= 1;
             ++launched;
             if (prm->tol > 0 && (k + 1) % check_every == 0) {
-                MVS_TRY_CUDA(launch_dependent(energy_kernel, dim3(kEnergyBlocks), dim3(EB), 0, st, L.T11, L.T12,
+                MVS_TRY_CUDA(launch_dependent(energy_kernel, dim3(energy_blocks(n)), dim3(EB), 0, st, L.T11, L.T12,
                                               L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V, prm->lambda,
-                                              prm->alpha0, prm->alpha1, L.partial, L.ctl));
-                MVS_TRY_CUDA(launch_dependent(energy_check_kernel, dim3(1), dim3(EB), 0, st, L.partial,
-                                              kEnergyBlocks, L.energy, L.ctl, prm->tol, launched));
+                                              prm->alpha0, prm->alpha1, L.partial, L.energy, L.ctl, prm->tol,
+                                              launched));
             }
             if (launched >= cap) {
                 done = true;
@@ -1486,9 +1482,9 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     }
     if (!rc && energy_out && energy_at != total) {
         // energy of the final iterate for callers that ask for it
-        energy_kernel<<<kEnergyBlocks, EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V,
-                                                   prm->lambda, prm->alpha0, prm->alpha1, L.partial, nullptr);
-        sum_partials_kernel<<<1, EB, 0, st>>>(L.partial, kEnergyBlocks, L.energy);
+        energy_kernel<<<energy_blocks(n), EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h,
+                                                      V, prm->lambda, prm->alpha0, prm->alpha1, L.partial, L.energy,
+                                                      L.ctl, 0.0, total);
         cudaMemcpyAsync(h_energy, L.energy, sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = set_error(MVS_ERR_CUDA, "tgv2 energy: %s", cudaGetErrorString(e));
