@@ -147,8 +147,52 @@ def main(only=None):
         print(f.name, f.stat().st_size)
 
 
+def real_frame_case(name, n_src=4, factor=4, n_planes=64, win=5, znear=0.1, zfar=1.0):
+    """The reference's own sample frames (src/PlaneSweep/im0..9.png with
+    Calibration.txt), grey as the GUI converts them (pclviewer.cpp:870-885,
+    weights defines.h:19-21), box-downsampled by `factor` and rounded to 8 bits
+    so the fixture stays small; K from the calibration line, scaled to the
+    smaller image; the poses as the GUI passes them (pclviewer.cpp:346-405).
+    Outputs of the reference's own kernels: the sweep with its float plane
+    loop, the TV-L1 denoise of that depthmap, and TGV2 from it."""
+    from PIL import Image
+    src_dir = pathlib.Path("/root/reference/src/PlaneSweep")
+    lines = (src_dir / "Calibration.txt").read_text().splitlines()
+    fx, fy, cx, cy, sk = (float(x) for x in lines[0].split())
+    W0, H0 = 640, 480
+    K0 = np.array([[fx * W0, (1 - sk) * W0, cx * W0], [0, fy * H0, cy * H0], [0, 0, 1]])
+    poses = []
+    for k, ln in enumerate(lines):
+        if ln.startswith("Transform"):
+            m = np.array([[float(x) for x in lines[k + r].split()] for r in (1, 2, 3)])
+            poses.append((m[:, :3].astype(np.float32), m[:, 3].astype(np.float32)))
+    imgs = []
+    for i in range(n_src + 1):
+        rgb = np.asarray(Image.open(src_dir / f"im{i}.png").convert("RGB"), np.float64)
+        gray = (0.2989 * rgb[..., 0] + 0.1140 * rgb[..., 2] + 0.5870 * rgb[..., 1]).astype(np.float32)
+        h, w = gray.shape[0] // factor, gray.shape[1] // factor
+        g = gray[:h * factor, :w * factor].reshape(h, factor, w, factor).mean(axis=(1, 3))
+        imgs.append(np.clip(np.rint(g), 0, 255).astype(np.uint8))
+    # 1-based pixel centres: full-resolution X = factor * X' - (factor - 1) / 2
+    S = np.array([[1 / factor, 0, (factor - 1) / (2 * factor)], [0, 1 / factor, (factor - 1) / (2 * factor)], [0, 0, 1]])
+    K = (S @ K0).astype(np.float32)
+    ref, srcs = imgs[0].astype(np.float32), [im.astype(np.float32) for im in imgs[1:]]
+    Rref, tref = poses[0]
+    src_poses = poses[1:n_src + 1]
+    r = po.ref_sweep(ref, srcs, K, Rref, tref, src_poses, None, win, znear=znear, zfar=zfar, nplanes=n_planes)
+    planes = po.plane_list(znear, zfar, n_planes)
+    den, _ = po.ref_tvl1_denoise(ref, r["depth"], znear, zfar, niters=50)
+    tgv, _ = po.ref_tgv(ref, srcs, K, Rref, tref, src_poses, niters=40, warps=2, u_init=r["depth"])
+    np.savez_compressed(HERE / f"{name}.npz", images=np.stack(imgs), K=K, Rref=Rref, tref=tref,
+                        Rsrc=np.stack([p[0] for p in src_poses]), tsrc=np.stack([p[1] for p in src_poses]),
+                        planes=planes, win=win, znear=znear, zfar=zfar, n_planes=n_planes,
+                        depth=r["depth"], label=po.labels_from_depth(r["vdepth"], planes).astype(np.int16),
+                        denoised=den, tgv=tgv)
+
+
 CASES = {
     "tgv_sparse": lambda: tgv_sparse_case("tgv_sparse", seed=51, w=48, h=40, niters=60, frac=0.1),
+    "real_frame": lambda: real_frame_case("real_frame"),
     "tgv_sparse_tensor": lambda: tgv_sparse_case("tgv_sparse_tensor", seed=52, w=37, h=29, niters=45, frac=0.25,
                                                  alpha0=1.3, alpha1=0.9, tau=0.05, sigma=2.0, theta=0.5, beta=2.5,
                                                  gamma=0.7),

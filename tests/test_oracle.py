@@ -197,3 +197,21 @@ def test_live_fusion_and_tgv_vs_reference():
     sr = po.ref_tgv_sparse(fr.ref, d0, sp, 6.0, 11, beta=1.5, gamma=0.8, theta=0.7)
     so = po.tgv_sparse(fr.ref, d0, sp, 6.0, 11, beta=1.5, gamma=0.8, precision="f32")
     np.testing.assert_array_equal(sr, so)
+
+
+def test_real_frame_f32_bit_exact_vs_golden(golden):
+    """The reference's own sample frames (grey, downsampled): the f32 oracle
+    equals the reference's kernels on the sweep (its float plane loop), the
+    TV-L1 denoise of that depthmap and TGV2 from it."""
+    g = golden("real_frame")
+    ref, srcs = g["images"][0].astype(np.float32), [im.astype(np.float32) for im in g["images"][1:]]
+    poses = [(g["Rsrc"][i], g["tsrc"][i]) for i in range(len(srcs))]
+    H = po.homographies(g["K"], g["Rref"], g["tref"], poses, g["planes"], precision="f32")
+    o = po.sweep(ref, srcs, H, g["planes"], int(g["win"]), zfar=float(g["zfar"]), precision="f32")
+    np.testing.assert_array_equal(o["depth"], g["depth"])
+    np.testing.assert_array_equal(o["label"], g["label"])
+    den = po.tvl1_denoise(ref, g["depth"], float(g["znear"]), float(g["zfar"]), niters=50, precision="f32")
+    np.testing.assert_array_equal(den, g["denoised"])
+    u, _, _ = po.tgv2(ref, srcs, g["K"], g["Rref"], g["tref"], poses, niters=40, warps=2, u_init=g["depth"],
+                      precision="f32")
+    np.testing.assert_array_equal(u, g["tgv"])
