@@ -177,7 +177,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ray-cast box room)",
             "impl": "reference",
-            "config": {"workload": "C2 sweep: 640x480, 8 views, 256 inverse-depth planes over [0.4, 8] m, 9x9 NCC",
+            "config": {"workload": "sweep: 640x480, 8 views, 256 inverse-depth planes over [0.4, 8] m, 9x9 NCC",
                        "sample_per_step": sample},
             "cpu_baseline": {"value": tput, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": tput, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -312,7 +312,7 @@ def run_tgv_sparse(fr, dev, d_ref, wta_depth, peak_gbs, reference_gpu):
 
 
 def run_batched(args, dev, stream, flush, rank):
-    """the mixed 48-frame batch through mvs_batch (one graph launch per batch)."""
+    """The mixed 48-frame batch through mvs_batch (one graph launch per batch)."""
     import time
     import torch
     import mvs_b200 as M
@@ -518,9 +518,10 @@ def main():
             tgv_ms.append(a.elapsed_time(b))
     tgv_ms_frame = dist.max_over_ranks(statistics.mean(tgv_ms), dev) if tgv_ms else None
 
-    # --- learned warm start (configs[4]): network prediction from (WTA depth, cost, image), then
+    # --- learned warm start: network prediction from (WTA depth, cost, image), then
     #     TGV2 from it with the same linearisation (WTA depth), tolerance and cap, against plain
-    #     TGV2 from the WTA depth (the judge), averaged over held-out frames of configs[1] ---
+    #     TGV2 from the WTA depth (the baseline it is measured against), averaged over held-out
+    #     640x480, 8-view frames ---
     warm = None
     if tgv_ms and args.warm_start:
         from mvs_b200 import warmstart as WS
@@ -562,14 +563,14 @@ def main():
     if args.tgv_sparse and rank == 0:
         tgv_sparse = run_tgv_sparse(fr, dev, d_ref, wta_depth, peaks()[0], args.reference_gpu)
 
-    # --- batched uneven frames (configs[3]): 48 frames (320x240 / 640x480 rooms, 1242x375 street)
+    # --- batched uneven frames: 48 frames (320x240 / 640x480 rooms, 1242x375 street)
     #     with 64-256 planes, 4-8 views and 5x5-11x11 windows in one graph launch; the autotuner
     #     picks plane chunking, persistent CTAs per SM and item order ---
     batched = None
     if args.batch:
         batched = run_batched(args, dev, stream, flush, rank)
 
-    # --- TV-L1 histogram fusion (configs[2]): 256^3 voxels over a 5 m cube, 40 depthmaps of
+    # --- TV-L1 histogram fusion: 256^3 voxels over a 5 m cube, 40 depthmaps of
     #     640x480 with 1% depth noise and 2% outliers, 7 bins, 200 primal-dual iterations ---
     fusion = None
     if args.fusion:
@@ -700,7 +701,7 @@ def main():
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (bf16 cost volume)",
         "data": "synthetic: seeded ray-cast box room, 4-octave value noise (stands in for ICL-NUIM)",
-        "config": {"workload": "C2 sweep: 640x480, 8 views, 256 inverse-depth planes over [0.4, 8] m, 9x9 NCC, "
+        "config": {"workload": "sweep: 640x480, 8 views, 256 inverse-depth planes over [0.4, 8] m, 9x9 NCC, "
                                "compensated moments, BF16 cost volume + WTA",
                    "per_rank_frames_per_step": 1, "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{ws}"},

@@ -1,6 +1,6 @@
 /* Driver for the reference's own CUDA kernels on the GPU (oracle/_ref/libmvs_ref_gpu.so).
  *
- * BASELINE AND TEST INFRASTRUCTURE ONLY.  Linked with the reference's
+ * REFERENCE-GPU TIMING AND TEST INFRASTRUCTURE ONLY.  Linked with the reference's
  * kernels.cu and TGV2_kernels.cu, compiled unchanged for sm_100a where they
  * lie in the reference tree (oracle/Makefile, target ref_gpu).  The functions
  * replay the call sequences of PlaneSweep::RunAlgorithm / PlaneSweepThread

@@ -7,7 +7,7 @@ image) and its converged TGV2 primal (u, v).  A U-Net (mvs_b200.Unet, tensor
 core kernels) learns the map; at run time its prediction starts TGV2
 (mvs_tgv2_run_warm) with the data term still linearised at the winner-take-all
 depth, so the warm and plain runs minimise the same energy and the plain run
-stays the judge (and the fallback) of the energy the warm start reaches.
+is what the warm start's time and final energy are measured against.
 
     python -m mvs_b200.warmstart train --scenes 2000 --out weights.npz
 
