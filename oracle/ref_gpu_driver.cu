@@ -5,8 +5,9 @@
  * lie in the reference tree (oracle/Makefile, target ref_gpu).  The functions
  * replay the call sequences of PlaneSweep::RunAlgorithm / PlaneSweepThread
  * (planesweep.cpp:74-259), PlaneSweep::TGV (planesweep.cpp:381-536) and
- * PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674) on device images, exactly as ref_driver.cpp replays them on host images for
- * the CPU build: the reference's wrappers, kernels and Matrix3D arithmetic,
+ * PlaneSweep::TGVdenoiseFromSparse (planesweep.cpp:596-674) on device images,
+ * exactly as ref_driver.cpp replays them on host images for the CPU build:
+ * the reference's wrappers, kernels and Matrix3D arithmetic,
  * one launch per wrapper call.  Buffers are allocated before the timed
  * region; buffers the reference leaves uninitialised are zero-filled.
  */
