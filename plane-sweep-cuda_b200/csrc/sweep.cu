@@ -7,8 +7,8 @@
 //       memory (homography + bilinear, the arithmetic of
 //       transform_indexes_kernel / bilinear_interpolation_kernel_GPU,
 //       kernels.cu:4-44; mirrored halo as windowed_mean_*, kernels.cu:203-229),
-//   A1  forms per-column window sums of w, w^2 and ref*w (64 columns x 4
-//       strips of 8 rows, one per thread; ref values stay in registers),
+//   A1  forms per-column window sums of w, w^2 and ref*w (72 columns x 3
+//       strips of 11 rows, one per thread),
 //   B   forms the row sums, the NCC (calcNCC_kernel, kernels.cu:46-64) and
 //       keeps the running best per pixel in registers (update_arrays_kernel,
 //       kernels.cu:66-82: strictly greater wins, so ties keep the earlier
@@ -33,6 +33,7 @@
 //                           windows, such as the zero fill outside the source,
 //                           then give NCC 0 exactly as in exact arithmetic.
 #include <math.h>
+#include <stddef.h>
 
 #include "common.cuh"
 
@@ -40,20 +41,39 @@ namespace mvs {
 namespace {
 
 constexpr int THREADS = 256;
-constexpr int TH = 32;       // output rows per tile
-constexpr int RWMAX = 64;    // region columns held in shared memory
-constexpr int CSP = 72;      // row pitch of the column-sum arrays (bank spread)
+constexpr int TH = 32;        // output rows per tile
+constexpr int RWMAX = 72;     // region columns held in shared memory
+constexpr int RHMAX = TH + 15;   // region rows of the largest window (15), plus the row the last A1 strip reads past it
+// Row pitch of the column-sum and moment arrays.  Pass B gives the 8 lanes of
+// a quarter warp 8 consecutive rows at one column: 76 = 12 (mod 32) floats
+// puts their 16-byte words on 8 distinct groups of 4 banks.
+constexpr int CSP = 76;
+constexpr int STRIP = 11;     // output rows per pass-A1 thread (the last strip has 10)
 
 template <int WIN>
 struct Geo {
     static constexpr int R = WIN / 2;
-    static constexpr int TW = ((RWMAX - 2 * R) / 8) * 8;  // output columns
+    static constexpr int TW = ((RWMAX - 2 * R) / 8) * 8;  // output columns: 64 up to 9x9, 56 above
     static constexpr int RUN = TW / 8;                     // outputs per thread in pass B
     static constexpr int RW = TW + 2 * R;                  // region columns used
     static constexpr int RH = TH + 2 * R;                  // region rows
-    static constexpr int SROWS = 8 + 2 * R;                // region rows per pass-A1 strip
-    static_assert(RW <= RWMAX, "region too wide");
+    // passes A0 / A1: three threads per region column (216 of the 256 at
+    // 72 columns); A0 thread (c, s) warps rows s, s + 3, ...; A1 thread
+    // (c, s) forms the column sums of output rows [11 s, 11 s + 11)
+    static constexpr int COLT = 3 * RW;
+    static constexpr int A0ROWS = (RH + 2) / 3;
+    static constexpr int SROWS = STRIP + 2 * R;            // region rows per pass-A1 strip
+    static_assert(RW <= RWMAX && RH <= RHMAX && COLT <= THREADS, "region too large");
+    static_assert(3 * STRIP >= TH && 2 * STRIP < TH, "three strips cover the tile");
+    static_assert(2 * STRIP + SROWS <= RHMAX, "strip reads stay inside the region arrays");
 };
+
+// pass B thread -> (output row, run of RUN columns): the 8 lanes of a
+// quarter warp take 8 consecutive rows of one run, so their 16-byte loads
+// of a run fall on distinct banks (CSP above); a warp stores 8 rows x 32
+// contiguous cost values.
+__device__ __forceinline__ int b_row() { return (int)(threadIdx.x & 7) + 8 * (int)(threadIdx.x >> 6); }
+__device__ __forceinline__ int b_seg() { return (int)(threadIdx.x >> 3) & 7; }
 
 struct SweepArgs {
     const float *ref;
@@ -72,29 +92,47 @@ struct SweepArgs {
 
 // ---- pass A0: warp the region into shared memory ------------------------------
 
-// Thread t always owns region column rx = t & 63 and rows (t >> 6) + 4k, so its
-// pixel column X and its CELLS pixel rows Y_k (mirrored at the image border)
+// Thread (c, s) = (t % RW, t / RW) always owns region column c and rows s + 3k,
+// so its pixel column X and its pixel rows Y_k (mirrored at the image border)
 // are fixed for the whole CTA: the rows sit in shared memory (Yc), and per
 // plane only the X-dependent part of H*(X, Y, 1) is formed once (COMPENSATED;
 // the REFERENCE path keeps the reference's dot-product order).  Cells are processed in
 // batches -- coordinates, then all gathers, then the interpolation -- so each
 // thread keeps several independent L1/L2 gathers in flight.
-template <int WIN>
-struct A0Cells {
-    static constexpr int CELLS = (Geo<WIN>::RH * RWMAX + THREADS - 1) / THREADS;
-};
 
-// ---- pass B: row sums of the three column-sum arrays ------------------------------
-// thread -> (row y = t >> 3, segment g = t & 7 of RUN outputs)
+// ---- pass B: row sums of one column-sum array --------------------------------------
+
+// The RUN + 2R column sums that thread (b_row, b_seg) reads: 16-byte loads
+// when a run is a multiple of 4 (the rows sit at a 16-byte pitch and the runs
+// start on multiples of 8 floats; the last word may reach past the region's
+// used columns into the row's padding, whose values are never used).
+template <int N, int RUN>
+__device__ __forceinline__ void load_run(const float *row, float *v)
+{
+    if constexpr (RUN % 4 == 0) {
+        const float4 *q = reinterpret_cast<const float4 *>(row);
+#pragma unroll
+        for (int i = 0; i < (N + 3) / 4; ++i) {
+            const float4 f = q[i];
+            v[4 * i] = f.x;
+            if (4 * i + 1 < N) v[4 * i + 1] = f.y;
+            if (4 * i + 2 < N) v[4 * i + 2] = f.z;
+            if (4 * i + 3 < N) v[4 * i + 3] = f.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = row[i];
+    }
+}
 
 template <int WIN, int MOM>
-__device__ __forceinline__ void row_sums(float (*CS)[TH][CSP], int q, float *out)
+__device__ __forceinline__ void row_sums(const float (*CSq)[CSP], float *out)
 {
     using G = Geo<WIN>;
-    const int y = threadIdx.x >> 3, g = threadIdx.x & 7;
-    float v[G::RUN + 2 * G::R];
-#pragma unroll
-    for (int i = 0; i < G::RUN + 2 * G::R; ++i) v[i] = CS[q][y][g * G::RUN + i];
+    constexpr int NV = G::RUN + 2 * G::R;
+    static_assert(G::RUN % 4 != 0 || 7 * G::RUN + 4 * ((NV + 3) / 4) <= CSP, "run loads stay inside a row");
+    float v[NV];
+    load_run<NV, G::RUN>(CSq[b_row()] + b_seg() * G::RUN, v);
     if (MOM == MVS_MOMENTS_REFERENCE) {
         // windowed_mean_row_kernel: direct sum in window order, then / winsize
 #pragma unroll
@@ -118,62 +156,65 @@ __device__ __forceinline__ void row_sums(float (*CS)[TH][CSP], int q, float *out
 }
 
 // Rounding bound of n*Sxx - Sx^2 for the compensated sums, as a multiple of
-// Sxx: about 3 n eps per addition, with 2*WIN + 26 additions along the
-// column and row passes.  Windows at or below it count as flat.
+// Sxx: about 3 n eps per addition, with WIN + 2 (STRIP - 1) additions along
+// a column strip and WIN + 2 (RUN - 1) along a row run.  Windows at or below
+// it count as flat.
 template <int WIN>
 __device__ __forceinline__ constexpr float flat_kappa()
 {
-    return 3.f * (float)(WIN * WIN) * (float)(2 * WIN + 26) * 5.9604645e-8f;
+    return 3.f * (float)(WIN * WIN) * (float)(2 * WIN + 2 * (STRIP - 1) + 2 * (Geo<WIN>::RUN - 1)) * 5.9604645e-8f;
 }
 
 // Reference moments of the tile, once per CTA: in REFERENCE mode the mean and
 // the naive std (calculate_STD_kernel, kernels.cu:103-120) of the reference
 // window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2 (0 if flat).
 template <int WIN, int MOM>
-__device__ void ref_moments(float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float *rm, float *rs)
+__device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float (*RM)[CSP],
+                            float (*RS)[CSP])
 {
     using G = Geo<WIN>;
-    {
-        const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
-        if (c < G::RW) {
+    if (threadIdx.x < G::COLT) {
+        const int c = threadIdx.x % G::RW, s = threadIdx.x / G::RW;
+        const int r0 = STRIP * s;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                float s1 = 0.f, s2 = 0.f;
+        for (int k = 0; k < STRIP; ++k) {
+            if (r0 + k >= TH) break;
+            float s1 = 0.f, s2 = 0.f;
 #pragma unroll
-                for (int i = 0; i < WIN; ++i) {
-                    if (MOM == MVS_MOMENTS_REFERENCE) {
-                        const float x = Rt[8 * s + k + i][c];
-                        s1 = s1 + x;
-                        s2 = s2 + x * x;
-                    } else {
-                        const float x = Rt[8 * s + k + i][c] - shift;
-                        s1 += x;
-                        s2 = fmaf(x, x, s2);
-                    }
-                }
+            for (int i = 0; i < WIN; ++i) {
                 if (MOM == MVS_MOMENTS_REFERENCE) {
-                    s1 = s1 / (float)WIN;
-                    s2 = s2 / (float)WIN;
+                    const float x = Rt[r0 + k + i][c];
+                    s1 = s1 + x;
+                    s2 = s2 + x * x;
+                } else {
+                    const float x = Rt[r0 + k + i][c] - shift;
+                    s1 += x;
+                    s2 = fmaf(x, x, s2);
                 }
-                CS[0][8 * s + k][c] = s1;
-                CS[1][8 * s + k][c] = s2;
             }
+            if (MOM == MVS_MOMENTS_REFERENCE) {
+                s1 = s1 / (float)WIN;
+                s2 = s2 / (float)WIN;
+            }
+            CS[0][r0 + k][c] = s1;
+            CS[1][r0 + k][c] = s2;
         }
     }
     __syncthreads();
     float m[G::RUN], q[G::RUN];
-    row_sums<WIN, MOM>(CS, 0, m);
-    row_sums<WIN, MOM>(CS, 1, q);
+    row_sums<WIN, MOM>(CS[0], m);
+    row_sums<WIN, MOM>(CS[1], q);
+    const int y = b_row(), x = b_seg() * G::RUN;
 #pragma unroll
     for (int j = 0; j < G::RUN; ++j) {
         if (MOM == MVS_MOMENTS_REFERENCE) {
             const float var = q[j] - m[j] * m[j];
-            rm[j] = m[j];
-            rs[j] = var > 0 ? sqrtf(var) : 0.f;
+            RM[y][x + j] = m[j];
+            RS[y][x + j] = var > 0 ? sqrtf(var) : 0.f;
         } else {
             const float v = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
-            rm[j] = m[j];
-            rs[j] = v > flat_kappa<WIN>() * q[j] ? v : 0.f;
+            RM[y][x + j] = m[j];
+            RS[y][x + j] = v > flat_kappa<WIN>() * q[j] ? v : 0.f;
         }
     }
     __syncthreads();
@@ -199,7 +240,7 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
 
 // Shared-memory layout of one CTA.
 struct __align__(16) Smem {
-    float Wt[TH + 16][RWMAX];      // warped region (reference region at start)
+    float Wt[RHMAX][RWMAX];        // warped region (reference region at start)
     float CS[3][TH][CSP];          // column sums
     float Hm[9];
     float red[THREADS / 32];
@@ -251,14 +292,18 @@ __device__ __forceinline__ float tile_shift(Smem &S)
 
 struct __align__(16) AggSmem {
     Smem S;
-    float Rf[TH + 16][RWMAX];   // reference region (shifted in the compensated mode)
-    float Yc[TH + 16];          // region row coordinates (1-based, mirrored)
-    // reference window sums / means and n^2 var / std per output pixel; rows
-    // at the CSP pitch, so the four rows one warp reads in pass B sit on
-    // distinct banks (at a 64-float pitch they were a 4-way conflict)
+    float Rf[RHMAX][RWMAX];     // reference region (shifted in the compensated mode)
+    // reference window sums / means and n^2 var / std per output pixel, at
+    // the CSP pitch and 16-byte aligned: pass B reads them as it reads CS
     float RM[TH][CSP];
     float RS[TH][CSP];
+    float Yc[RHMAX];            // region row coordinates (1-based, mirrored)
 };
+// three CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
+static_assert(3 * (sizeof(AggSmem) + 1024) <= 228 * 1024, "three CTAs per SM");
+static_assert(offsetof(AggSmem, RM) % 16 == 0 && offsetof(AggSmem, RS) % 16 == 0 &&
+                  offsetof(AggSmem, S.CS) % 16 == 0 && (CSP * sizeof(float)) % 16 == 0,
+              "16-byte run loads");
 
 // Each source pixel's 2x2 bilinear neighbourhood (x, x+1 on rows y, y+1) as
 // one aligned 16-byte word, so that a warp sample is one load instead of four
@@ -279,35 +324,45 @@ __global__ void quad_kernel(const float *__restrict__ src, int V, int w, int h, 
     }
 }
 
+// 1.5 * 2^23: for 0 <= x < 2^22, x + C rounded down is C + floor(x) exactly,
+// an integer in [2^23, 2^24) whose low mantissa bits are floor(x); the
+// subtraction C then gives floor(x) as a float, also exactly.  Floors on the
+// FMA pipe instead of the conversion unit (a standard magic-number floor).
+constexpr float kFloorMagic = 12582912.f;
+constexpr int kFloorMagicBits = 0x4B400000;
+
 // pass A0 with the row coordinates from shared memory; `quad` (may be null)
-// holds the source's 2x2 neighbourhoods
+// holds the source's 2x2 neighbourhoods.  COMPENSATED stores the samples
+// shifted by `shift`.
 template <int WIN, int MOM>
 __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src,
                                              const float4 *__restrict__ quad, int w, int h, const float *Hm, float X,
-                                             const float *Yc)
+                                             const float *Yc, float shift)
 {
     using G = Geo<WIN>;
-    constexpr int CELLS = A0Cells<WIN>::CELLS;
+    constexpr int CELLS = G::A0ROWS;
     constexpr int BATCH = 4;
-    const int rx = threadIdx.x & 63, rb = threadIdx.x >> 6;
-    if (rx >= G::RW) return;
+    if (threadIdx.x >= G::COLT) return;
+    const int rx = threadIdx.x % G::RW, rb = threadIdx.x / G::RW;
     const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
-    // fx + 1 <= w - 1 is fx <= w - 2 for the integer-valued fx (also for
-    // |fx| >= 2^24, inf and NaN, where both forms agree)
-    const float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
+    // floor(xs) in [0, w - 2] is 0 <= xs < w - 1.  xs is never -0 (a sum
+    // x + (-1) that is exactly zero rounds to +0), and non-negative floats,
+    // +inf and +NaN order like their bit patterns while negative ones (and
+    // -NaN) have the sign bit, so the test is one unsigned compare per axis.
+    const unsigned wm1 = __float_as_uint((float)(w - 1)), hm1 = __float_as_uint((float)(h - 1));
 #pragma unroll
     for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
         float fa[BATCH], fb[BATCH];
-        int off[BATCH];
+        unsigned off[BATCH];   // read only where ok: unsigned, so the unused values wrap harmlessly
         bool ok[BATCH];
 #pragma unroll
         for (int j = 0; j < BATCH; ++j) {
             const int k = k0 + j;
             ok[j] = false;
-            off[j] = 0;
             fa[j] = fb[j] = 0.f;
-            if (k < CELLS && rb + 4 * k < G::RH) {
-                const float Y = Yc[rb + 4 * k];
+            off[j] = 0u;
+            if (k < CELLS && rb + 3 * k < G::RH) {
+                const float Y = Yc[rb + 3 * k];
                 float xs, ys;
                 if (MOM == MVS_MOMENTS_REFERENCE) {
                     const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
@@ -322,13 +377,12 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
                     xs = fmaf(q0, rz, -1.f);
                     ys = fmaf(q1, rz, -1.f);
                 }
-                const float fx = floorf(xs), fy = floorf(ys);
-                ok[j] = fx >= 0.f && fy >= 0.f && fx <= wm2 && fy <= hm2;
-                if (ok[j]) {
-                    fa[j] = xs - fx;
-                    fb[j] = ys - fy;
-                    off[j] = (int)fy * w + (int)fx;
-                }
+                ok[j] = __float_as_uint(xs) < wm1 && __float_as_uint(ys) < hm1;
+                const float tx = __fadd_rd(xs, kFloorMagic), ty = __fadd_rd(ys, kFloorMagic);
+                fa[j] = xs - (tx - kFloorMagic);
+                fb[j] = ys - (ty - kFloorMagic);
+                off[j] = (__float_as_uint(ty) - (unsigned)kFloorMagicBits) * (unsigned)w +
+                         (__float_as_uint(tx) - (unsigned)kFloorMagicBits);
             }
         }
         float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
@@ -360,75 +414,80 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
 #pragma unroll
         for (int j = 0; j < BATCH; ++j) {
             const int k = k0 + j;
-            if (k >= CELLS || rb + 4 * k >= G::RH) continue;
-            float v = 0.f;
-            if (ok[j]) {
-                const float a = fa[j], b = fb[j];
-                if (MOM == MVS_MOMENTS_REFERENCE) {
-                    const float t1 = a * d01[j] + (1 - a) * d00[j];
-                    const float t2 = a * d11[j] + (1 - a) * d10[j];
-                    v = b * t2 + (1 - b) * t1;
-                } else {
-                    const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
-                    const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
-                    v = fmaf(b, t2 - t1, t1);
-                }
+            if (k >= CELLS || rb + 3 * k >= G::RH) continue;
+            const float a = fa[j], b = fb[j];
+            float v;
+            if (MOM == MVS_MOMENTS_REFERENCE) {
+                const float t1 = a * d01[j] + (1 - a) * d00[j];
+                const float t2 = a * d11[j] + (1 - a) * d10[j];
+                v = ok[j] ? b * t2 + (1 - b) * t1 : 0.f;
+            } else {
+                const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
+                const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
+                v = (ok[j] ? fmaf(b, t2 - t1, t1) : 0.f) - shift;
             }
-            Wt[rb + 4 * k][rx] = v;
+            Wt[rb + 3 * k][rx] = v;
         }
     }
 }
 
-// pass A1 with the reference column read from shared memory
+// pass A1 with the reference column read from shared memory: thread (c, s)
+// forms the column sums of w, w^2 and ref*w for output rows [11 s, 11 s + 11)
+// (COMPENSATED: Wt and Rf hold shifted values already)
 template <int WIN, int MOM>
-__device__ __forceinline__ void pass_a1_rows(float (*Wt)[RWMAX], float (*CS)[TH][CSP], float (*Rf)[RWMAX],
-                                             float shift)
+__device__ __forceinline__ void pass_a1_rows(const float (*Wt)[RWMAX], float (*CS)[TH][CSP],
+                                             const float (*Rf)[RWMAX])
 {
     using G = Geo<WIN>;
-    const int c = threadIdx.x & 63, s = threadIdx.x >> 6;
-    if (c >= G::RW) return;
+    if (threadIdx.x >= G::COLT) return;
+    const int c = threadIdx.x % G::RW, s = threadIdx.x / G::RW;
+    const int r0 = STRIP * s;
+    const bool full = r0 + STRIP <= TH;   // the last strip has TH - 2 STRIP rows
     float wv[G::SROWS];
 #pragma unroll
-    for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[8 * s + i][c];
+    for (int i = 0; i < G::SROWS; ++i) wv[i] = Wt[r0 + i][c];
     if (MOM == MVS_MOMENTS_REFERENCE) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < STRIP; ++k) {
+            if (k == STRIP - 1 && !full) break;
             float s1 = 0.f, s2 = 0.f, s12 = 0.f;
 #pragma unroll
             for (int i = 0; i < WIN; ++i) {
                 const float x = wv[k + i];
                 s1 = s1 + x;
                 s2 = s2 + x * x;
-                s12 = s12 + Rf[8 * s + k + i][c] * x;
+                s12 = s12 + Rf[r0 + k + i][c] * x;
             }
             s1 = s1 / (float)WIN;
             s2 = s2 / (float)WIN;
             s12 = s12 / (float)WIN;
-            CS[0][8 * s + k][c] = s1;
-            CS[1][8 * s + k][c] = s2;
-            CS[2][8 * s + k][c] = s12;
+            CS[0][r0 + k][c] = s1;
+            CS[1][r0 + k][c] = s2;
+            CS[2][r0 + k][c] = s12;
         }
     } else {
+        float rf[G::SROWS];
 #pragma unroll
-        for (int i = 0; i < G::SROWS; ++i) wv[i] -= shift;
+        for (int i = 0; i < G::SROWS; ++i) rf[i] = Rf[r0 + i][c];
         float s1 = 0.f, s2 = 0.f, s12 = 0.f;
 #pragma unroll
         for (int i = 0; i < WIN; ++i) {
             s1 += wv[i];
             s2 = fmaf(wv[i], wv[i], s2);
-            s12 = fmaf(Rf[8 * s + i][c], wv[i], s12);
+            s12 = fmaf(rf[i], wv[i], s12);
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < STRIP; ++k) {
+            if (k == STRIP - 1 && !full) break;
             if (k > 0) {
                 const float xn = wv[k + WIN - 1], xo = wv[k - 1];
                 s1 = (s1 + xn) - xo;
                 s2 = fmaf(-xo, xo, fmaf(xn, xn, s2));
-                s12 = fmaf(-Rf[8 * s + k - 1][c], xo, fmaf(Rf[8 * s + k + WIN - 1][c], xn, s12));
+                s12 = fmaf(-rf[k - 1], xo, fmaf(rf[k + WIN - 1], xn, s12));
             }
-            CS[0][8 * s + k][c] = s1;
-            CS[1][8 * s + k][c] = s2;
-            CS[2][8 * s + k][c] = s12;
+            CS[0][r0 + k][c] = s1;
+            CS[1][r0 + k][c] = s2;
+            CS[2][r0 + k][c] = s12;
         }
     }
 }
@@ -452,25 +511,20 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    {
-        float rm[G::RUN], rs[G::RUN];
-        ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
-        const int yy = threadIdx.x >> 3, g = threadIdx.x & 7;
-#pragma unroll
-        for (int j = 0; j < G::RUN; ++j) {
-            A.RM[yy][g * G::RUN + j] = rm[j];
-            A.RS[yy][g * G::RUN + j] = rs[j];
-        }
-    }
-    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x & 63), w) + 1);
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
 
-    const int y = y0 + (threadIdx.x >> 3);
-    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
-    const int ly = threadIdx.x >> 3, lx = (threadIdx.x & 7) * G::RUN;
+    const int ly = b_row(), lx = b_seg() * G::RUN;
+    const int y = y0 + ly, xb = x0 + lx;
+    // the run's cost values as one 16-byte store: 8 per run, every row a
+    // multiple of 8 values, the run inside the frame, the volume 16-byte aligned
+    const bool vec_cost = G::RUN == 8 && a.cost && (w & 7) == 0 && xb + 8 <= w &&
+                          ((uintptr_t)a.cost & 15) == 0;
     uint32_t best[G::RUN];   // (bf16 cost bits << 16) | plane
 #pragma unroll
     for (int j = 0; j < G::RUN; ++j) best[j] = 0xffffffffu;
     const float invV = 1.f / (float)a.V;
+    const float sh = MOM == MVS_MOMENTS_REFERENCE ? 0.f : shift;
     const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
     for (int p = p0; p < p1; ++p) {
         float acc[G::RUN];
@@ -483,28 +537,43 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
 #pragma unroll
             for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
             pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, a.quad ? a.quad + (size_t)view * n : nullptr, w, h,
-                                   Hm, Xcol, A.Yc);
+                                   Hm, Xcol, A.Yc, sh);
             __syncthreads();
-            pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf, shift);
+            pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
             __syncthreads();
-            float s1[G::RUN], s2[G::RUN], s12[G::RUN];
-            row_sums<WIN, MOM>(S.CS, 0, s1);
-            row_sums<WIN, MOM>(S.CS, 1, s2);
-            row_sums<WIN, MOM>(S.CS, 2, s12);
+            float s1[G::RUN], s2[G::RUN], s12[G::RUN], rm[G::RUN], rs[G::RUN];
+            row_sums<WIN, MOM>(S.CS[0], s1);
+            row_sums<WIN, MOM>(S.CS[1], s2);
+            row_sums<WIN, MOM>(S.CS[2], s12);
+            load_run<G::RUN, G::RUN>(A.RM[ly] + lx, rm);
+            load_run<G::RUN, G::RUN>(A.RS[ly] + lx, rs);
 #pragma unroll
-            for (int j = 0; j < G::RUN; ++j)
-                acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], A.RM[ly][lx + j], A.RS[ly][lx + j], a.stdthresh);
+            for (int j = 0; j < G::RUN; ++j) acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
         }
+        uint16_t cb[G::RUN];
 #pragma unroll
         for (int j = 0; j < G::RUN; ++j) {
             // cost = 1 - mean NCC, clamped at 0 (rounding can push a perfect match
             // below 0; the stored bf16 bits then order like unsigned integers)
             float cf = fmaf(-acc[j], invV, 1.f);
             cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
-            const uint16_t cb = f2bf(cf);
-            const int x = xb + j;
-            if (a.cost && y < h && x < w) a.cost[(size_t)p * n + (size_t)y * w + x] = cb;
-            best[j] = min(best[j], ((uint32_t)cb << 16) | (uint32_t)p);
+            cb[j] = f2bf(cf);
+            best[j] = min(best[j], ((uint32_t)cb[j] << 16) | (uint32_t)p);
+        }
+        if (a.cost && y < h) {
+            uint16_t *row = a.cost + (size_t)p * n + (size_t)y * w + xb;
+            if (vec_cost) {
+                uint4 q;
+                q.x = (uint32_t)cb[0] | ((uint32_t)cb[1 % G::RUN] << 16);
+                q.y = (uint32_t)cb[2 % G::RUN] | ((uint32_t)cb[3 % G::RUN] << 16);
+                q.z = (uint32_t)cb[4 % G::RUN] | ((uint32_t)cb[5 % G::RUN] << 16);
+                q.w = (uint32_t)cb[6 % G::RUN] | ((uint32_t)cb[7 % G::RUN] << 16);
+                *reinterpret_cast<uint4 *>(row) = q;
+            } else {
+#pragma unroll
+                for (int j = 0; j < G::RUN; ++j)
+                    if (xb + j < w) row[j] = cb[j];
+            }
         }
     }
     if (y >= h) return;
@@ -551,18 +620,10 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    {
-        float rm[G::RUN], rs[G::RUN];
-        ref_moments<WIN, MOM>(S.Wt, S.CS, shift, rm, rs);
-        const int yy = threadIdx.x >> 3, g = threadIdx.x & 7;
-#pragma unroll
-        for (int j = 0; j < G::RUN; ++j) {
-            A.RM[yy][g * G::RUN + j] = rm[j];
-            A.RS[yy][g * G::RUN + j] = rs[j];
-        }
-    }
-    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x & 63), w) + 1);
-    const int ly = threadIdx.x >> 3, lx = (threadIdx.x & 7) * G::RUN;
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
+    const int ly = b_row(), lx = b_seg() * G::RUN;
+    const float sh = MOM == MVS_MOMENTS_REFERENCE ? 0.f : shift;
 
     float best[G::RUN];
     int lab[G::RUN];
@@ -579,17 +640,19 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         float Hm[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
-        pass_a0_rows<WIN, MOM>(S.Wt, src, quad, w, h, Hm, Xcol, A.Yc);
+        pass_a0_rows<WIN, MOM>(S.Wt, src, quad, w, h, Hm, Xcol, A.Yc, sh);
         __syncthreads();
-        pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf, shift);
+        pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
         __syncthreads();
-        float s1[G::RUN], s2[G::RUN], s12[G::RUN];
-        row_sums<WIN, MOM>(S.CS, 0, s1);
-        row_sums<WIN, MOM>(S.CS, 1, s2);
-        row_sums<WIN, MOM>(S.CS, 2, s12);
+        float s1[G::RUN], s2[G::RUN], s12[G::RUN], rm[G::RUN], rs[G::RUN];
+        row_sums<WIN, MOM>(S.CS[0], s1);
+        row_sums<WIN, MOM>(S.CS[1], s2);
+        row_sums<WIN, MOM>(S.CS[2], s12);
+        load_run<G::RUN, G::RUN>(A.RM[ly] + lx, rm);
+        load_run<G::RUN, G::RUN>(A.RS[ly] + lx, rs);
 #pragma unroll
         for (int j = 0; j < G::RUN; ++j) {
-            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], A.RM[ly][lx + j], A.RS[ly][lx + j], a.stdthresh);
+            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
             if (c > best[j]) {
                 best[j] = c;
                 lab[j] = p;
@@ -598,9 +661,9 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
     }
     // results: (ncc bits << 32) | ~plane, so that a 64-bit max keeps the
     // largest NCC and, among equal NCCs, the earliest plane.
-    const int y = y0 + (threadIdx.x >> 3);
+    const int y = y0 + ly;
     if (y >= h) return;
-    const int xb = x0 + (threadIdx.x & 7) * G::RUN;
+    const int xb = x0 + lx;
     unsigned long long *outp = a.packed + (size_t)view * w * h + (size_t)y * w;
 #pragma unroll
     for (int j = 0; j < G::RUN; ++j) {
