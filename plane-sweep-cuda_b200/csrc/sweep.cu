@@ -242,7 +242,7 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
 struct __align__(16) Smem {
     float Wt[RHMAX][RWMAX];        // warped region (reference region at start)
     float CS[3][TH][CSP];          // column sums
-    float Hm[9];
+    float Hm[2][9];                // homographies of this and the next (plane, view)
     float red[THREADS / 32];
 };
 
@@ -526,18 +526,29 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
     const float invV = 1.f / (float)a.V;
     const float sh = MOM == MVS_MOMENTS_REFERENCE ? 0.f : shift;
     const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
+    // Homographies double-buffered: thread k < 9 fetches element k of the next
+    // (plane, view) during pass A0 and the barrier that ends the pass publishes
+    // it, so a view takes two barriers.  Pass A0 of the next view needs no
+    // barrier before it: it writes only Wt, which pass A1 has finished reading.
+    if (threadIdx.x < 9 && p0 < p1) S.Hm[0][threadIdx.x] = ldg(a.H + (size_t)p0 * 9 + threadIdx.x);
+    __syncthreads();
+    int hb = 0;
     for (int p = p0; p < p1; ++p) {
         float acc[G::RUN];
 #pragma unroll
         for (int j = 0; j < G::RUN; ++j) acc[j] = 0.f;
         for (int view = 0; view < a.V; ++view) {
-            if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(a.H + ((size_t)view * a.P + p) * 9 + threadIdx.x);
-            __syncthreads();
             float Hm[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
+            for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[hb][k];
+            const bool last_view = view + 1 == a.V;
+            const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
+            float hn = 0.f;
+            if (threadIdx.x < 9 && np < p1) hn = ldg(a.H + ((size_t)nv * a.P + np) * 9 + threadIdx.x);
             pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, a.quad ? a.quad + (size_t)view * n : nullptr, w, h,
                                    Hm, Xcol, A.Yc, sh);
+            if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
+            hb ^= 1;
             __syncthreads();
             pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
             __syncthreads();
@@ -634,14 +645,20 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
     }
     const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
     const float *Hv = a.H + (size_t)view * a.P * 9;
+    // homographies double-buffered as in the aggregated tile: two barriers a plane
+    if (threadIdx.x < 9 && p0 < p1) S.Hm[0][threadIdx.x] = ldg(Hv + (size_t)p0 * 9 + threadIdx.x);
+    __syncthreads();
+    int hb = 0;
     for (int p = p0; p < p1; ++p) {
-        if (threadIdx.x < 9) S.Hm[threadIdx.x] = ldg(Hv + (size_t)p * 9 + threadIdx.x);
-        __syncthreads();   // Hm visible; previous plane's pass B finished with CS
         float Hm[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[k];
+        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[hb][k];
+        float hn = 0.f;
+        if (threadIdx.x < 9 && p + 1 < p1) hn = ldg(Hv + (size_t)(p + 1) * 9 + threadIdx.x);
         pass_a0_rows<WIN, MOM>(S.Wt, src, quad, w, h, Hm, Xcol, A.Yc, sh);
-        __syncthreads();
+        if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
+        hb ^= 1;
+        __syncthreads();   // Wt and the next homography visible; pass B of the previous plane done with CS
         pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
         __syncthreads();
         float s1[G::RUN], s2[G::RUN], s12[G::RUN], rm[G::RUN], rs[G::RUN];
