@@ -385,7 +385,7 @@ def run_batched(args, dev, stream, flush, rank):
            "tuning": {"planes_per_chunk": ppc, "ctas_per_sm": ctas,
                       "order": ["frame", "largest_first", "interleaved"][order]},
            "autotune_s": tune_s, "work_items": b.work_items,
-           "sequential_single_frame_ms": statistics.mean(seq), "launches_per_batch": 3,
+           "sequential_single_frame_ms": statistics.mean(seq), "launches_per_batch": 4,
            "planes": [sp.n_planes for sp in specs], "windows": [sp.window for sp in specs]}
     b.close()
     return out

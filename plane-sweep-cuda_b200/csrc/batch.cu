@@ -2,7 +2,8 @@
 // PlaneSweep handles one reference frame per call): many reference frames of
 // any size, view count, plane count and window go through one CUDA-graph
 // launch -- a timestamp kernel, one launch of FP64 homographies for every
-// (frame, view, plane) and one persistent sweep kernel over a work list of
+// (frame, view, plane), one launch building every frame's 2x2 source
+// neighbourhoods and one persistent sweep kernel over a work list of
 // (frame, tile, plane chunk) items (sweep.cu).  The aggregated mode (cost =
 // 1 - mean NCC over views, winner-take-all) is computed, with the moments the
 // caller picks.
@@ -270,7 +271,7 @@ int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, 
     const size_t o_frames = take(n * sizeof(BatchFrameDev)), o_cams = take(n * sizeof(BatchCamDev));
     const size_t o_hom = take((n + 1) * sizeof(int)), o_next = take(sizeof(unsigned)), o_t0 = take(8);
     const size_t o_done = take(n * 8);
-    std::vector<size_t> o_H(n), o_wta(n), o_tiles(n), o_fl(n);
+    std::vector<size_t> o_H(n), o_wta(n), o_tiles(n), o_fl(n), o_quad(n);
     for (int i = 0; i < n; ++i) {
         const mvs_batch_frame &f = frames[i];
         const int tw = sweep_tile_width(f.window), th = sweep_tile_height();
@@ -290,6 +291,8 @@ int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, 
         o_wta[i] = take((size_t)f.width * f.height * 8);
         o_tiles[i] = take((size_t)d.n_tiles * sizeof(unsigned));
         o_fl[i] = take(sizeof(unsigned));
+        // 2x2 source neighbourhoods, rebuilt from the sources at every launch
+        o_quad[i] = take((size_t)f.width * f.height * f.n_views * sizeof(float4));
     }
     b->n_hom = b->hom_off[n];
     cudaError_t e = cudaMalloc(&b->mem, off);
@@ -318,6 +321,7 @@ int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, 
         d.tile_left = (unsigned *)(b->mem + o_tiles[i]);
         d.frame_left = (unsigned *)(b->mem + o_fl[i]);
         d.done_ns = b->d_done + i;
+        d.quad = (const float4 *)(b->mem + o_quad[i]);
         BatchCamDev &c = b->cams[i];
         c.depths = f.d_depths;
         c.H = Hf;

@@ -306,20 +306,44 @@ static_assert(offsetof(AggSmem, RM) % 16 == 0 && offsetof(AggSmem, RS) % 16 == 0
               "16-byte run loads");
 
 // Each source pixel's 2x2 bilinear neighbourhood (x, x+1 on rows y, y+1) as
-// one aligned 16-byte word, so that a warp sample is one load instead of four
-// (the values, and so the arithmetic, are unchanged).  Only x <= w-2, y <= h-2
-// are ever read; the last row and column hold zeros.
-__global__ void quad_kernel(const float *__restrict__ src, int V, int w, int h, float4 *__restrict__ quad)
+// one aligned 16-byte word, so that a warp sample is one load instead of four.
+// Plain form (REFERENCE moments): the four values d00, d01, d10, d11, so the
+// reference's interpolation arithmetic is unchanged.  Difference form
+// (COMPENSATED): d00, d01 - d00, d10 - d00 and (d11 - d10) - (d01 - d00),
+// so the sample is d00 + a (d01 - d00) + b ((d10 - d00) + a (...)): three
+// fused multiply-adds.  Only x <= w-2, y <= h-2 are ever read; the last row
+// and column hold zeros.
+__device__ __forceinline__ float4 make_quad(const float *r, int w, bool diff)
+{
+    const float d00 = r[0], d01 = r[1], d10 = r[w], d11 = r[w + 1];
+    if (!diff) return make_float4(d00, d01, d10, d11);
+    return make_float4(d00, d01 - d00, d10 - d00, (d11 - d10) - (d01 - d00));
+}
+
+__global__ void quad_kernel(const float *__restrict__ src, int V, int w, int h, float4 *__restrict__ quad, int diff)
 {
     const size_t n = (size_t)w * h, total = n * V;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const size_t v = i / n, k = i - v * n;
         const int y = (int)(k / w), x = (int)(k - (size_t)y * w);
         float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (x < w - 1 && y < h - 1) {
-            const float *r = src + v * n + k;
-            q = make_float4(r[0], r[1], r[w], r[w + 1]);
-        }
+        if (x < w - 1 && y < h - 1) q = make_quad(src + v * n + k, w, diff != 0);
+        quad[i] = q;
+    }
+}
+
+// the same for every frame of a batch: grid (blocks, frames)
+__global__ void quad_batch_kernel(const BatchFrameDev *__restrict__ frames, int diff)
+{
+    const BatchFrameDev &f = frames[blockIdx.y];
+    float4 *quad = const_cast<float4 *>(f.quad);
+    const int w = f.w, h = f.h;
+    const size_t n = (size_t)w * h, total = n * f.V;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = i / n, k = i - v * n;
+        const int y = (int)(k / w), x = (int)(k - (size_t)y * w);
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (x < w - 1 && y < h - 1) q = make_quad(f.srcs + v * n + k, w, diff != 0);
         quad[i] = q;
     }
 }
@@ -331,10 +355,11 @@ __global__ void quad_kernel(const float *__restrict__ src, int V, int w, int h, 
 constexpr float kFloorMagic = 12582912.f;
 constexpr int kFloorMagicBits = 0x4B400000;
 
-// pass A0 with the row coordinates from shared memory; `quad` (may be null)
-// holds the source's 2x2 neighbourhoods.  COMPENSATED stores the samples
+// pass A0 with the row coordinates from shared memory; with QUAD, `quad` holds
+// the source's 2x2 neighbourhoods (difference form in COMPENSATED), else the
+// four samples are gathered from `src`.  COMPENSATED stores the samples
 // shifted by `shift`.
-template <int WIN, int MOM>
+template <int WIN, int MOM, bool QUAD>
 __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src,
                                              const float4 *__restrict__ quad, int w, int h, const float *Hm, float X,
                                              const float *Yc, float shift)
@@ -386,7 +411,7 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
             }
         }
         float d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
-        if (quad) {
+        if constexpr (QUAD) {
 #pragma unroll
             for (int j = 0; j < BATCH; ++j) {
                 d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
@@ -422,9 +447,11 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
                 const float t2 = a * d11[j] + (1 - a) * d10[j];
                 v = ok[j] ? b * t2 + (1 - b) * t1 : 0.f;
             } else {
-                const float t1 = fmaf(a, d01[j] - d00[j], d00[j]);
-                const float t2 = fmaf(a, d11[j] - d10[j], d10[j]);
-                v = (ok[j] ? fmaf(b, t2 - t1, t1) : 0.f) - shift;
+                // the difference form of the neighbourhood (as quad_kernel
+                // stores it), so both sources give the same roundings
+                float4 q = make_float4(d00[j], d01[j], d10[j], d11[j]);
+                if (!QUAD) q = make_float4(d00[j], d01[j] - d00[j], d10[j] - d00[j], (d11[j] - d10[j]) - (d01[j] - d00[j]));
+                v = (ok[j] ? fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)) : 0.f) - shift;
             }
             Wt[rb + 3 * k][rx] = v;
         }
@@ -545,8 +572,10 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
             float hn = 0.f;
             if (threadIdx.x < 9 && np < p1) hn = ldg(a.H + ((size_t)nv * a.P + np) * 9 + threadIdx.x);
-            pass_a0_rows<WIN, MOM>(S.Wt, a.srcs + (size_t)view * n, a.quad ? a.quad + (size_t)view * n : nullptr, w, h,
-                                   Hm, Xcol, A.Yc, sh);
+            if (a.quad)
+                pass_a0_rows<WIN, MOM, true>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc, sh);
+            else
+                pass_a0_rows<WIN, MOM, false>(S.Wt, a.srcs + (size_t)view * n, nullptr, w, h, Hm, Xcol, A.Yc, sh);
             if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
             hb ^= 1;
             __syncthreads();
@@ -655,7 +684,10 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[hb][k];
         float hn = 0.f;
         if (threadIdx.x < 9 && p + 1 < p1) hn = ldg(Hv + (size_t)(p + 1) * 9 + threadIdx.x);
-        pass_a0_rows<WIN, MOM>(S.Wt, src, quad, w, h, Hm, Xcol, A.Yc, sh);
+        if (quad)
+            pass_a0_rows<WIN, MOM, true>(S.Wt, nullptr, quad, w, h, Hm, Xcol, A.Yc, sh);
+        else
+            pass_a0_rows<WIN, MOM, false>(S.Wt, src, nullptr, w, h, Hm, Xcol, A.Yc, sh);
         if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
         hb ^= 1;
         __syncthreads();   // Wt and the next homography visible; pass B of the previous plane done with CS
@@ -1063,7 +1095,8 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     if (quad) {
         const size_t total = (size_t)n * d->n_views;
         const size_t blocks = (total + 255) / 256 < (size_t)16 * kSMs ? (total + 255) / 256 : (size_t)16 * kSMs;
-        quad_kernel<<<(int)blocks, 256, 0, st>>>(srcs, d->n_views, d->width, d->height, quad);
+        quad_kernel<<<(int)blocks, 256, 0, st>>>(srcs, d->n_views, d->width, d->height, quad,
+                                                 d->moments == MVS_MOMENTS_COMPENSATED);
         a.quad = quad;
     }
     if (d->mode == MVS_SWEEP_PER_VIEW) {
@@ -1098,6 +1131,8 @@ int sweep_batch_launch(const BatchFrameDev *frames, const uint4 *items, int n_it
     cudaStream_t st = (cudaStream_t)stream;
     batch_start_kernel<<<1, 1, 0, st>>>(next, t_start);
     if (n_hom > 0) homography_batch_kernel<<<ceil_div(n_hom, 128), 128, 0, st>>>(cams, hom_offsets, n_frames);
+    quad_batch_kernel<<<dim3(max(1, 4 * kSMs / max(1, n_frames)), n_frames), 256, 0, st>>>(
+        frames, moments == MVS_MOMENTS_COMPENSATED);
     const int sm = (int)sizeof(AggSmem);
     if (moments == MVS_MOMENTS_REFERENCE) {
         MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MVS_MOMENTS_REFERENCE>,
