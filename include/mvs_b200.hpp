@@ -284,6 +284,9 @@ protected:
     std::vector<float> viewbest;
     float lastms = 0.f;
     mvs::PlaneSweepImpl *impl;
+    /* the C-ABI image setters stage and upload the images in one pass */
+    friend int ::mvs_ps_set_reference(mvs_planesweep *, const float *, int32_t, int32_t, const float *, const float *);
+    friend int ::mvs_ps_set_sources(mvs_planesweep *, const float *, int32_t, const float *, const float *);
 
     void ConvertDepthtoUChar(const CamImage<float> &input, CamImage<uchar> &output);
     std::vector<float> planeDepths() const;

@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <new>
 #include <thread>
@@ -82,34 +83,55 @@ struct CopyPiece {
     void *dst;
     const void *src;
     size_t bytes;
+    void *dev = nullptr;   // if set: dst is page-locked and is uploaded here as it fills
 };
 
-void parallel_copy(const std::vector<CopyPiece> &pieces)
+// Upload granule: a thread stages this many bytes, then queues their
+// upload on the stream, so the copy engine starts after the first MB
+// instead of after the whole frame (256 KB granules made the 8 staging
+// threads wait on each other in the driver: 44 calls for an 11 MB frame).
+constexpr size_t kUploadChunk = (size_t)1 << 20;
+
+// Returns 0, or the first CUDA error of a queued upload.
+int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
 {
     size_t total = 0;
     for (const CopyPiece &c : pieces) total += c.bytes;
     const size_t min_part = (size_t)1 << 20;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int parts = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total / min_part));
+    std::atomic<int> err{0};
     auto run = [&](int k) {
         // part k copies bytes [k * total / parts, (k + 1) * total / parts) of the concatenation
         const size_t lo = total * k / parts, hi = total * (k + 1) / parts;
         size_t base = 0;
         for (const CopyPiece &c : pieces) {
             const size_t a = std::max(lo, base), b = std::min(hi, base + c.bytes);
-            if (a < b) stream_copy((char *)c.dst + (a - base), (const char *)c.src + (a - base), b - a);
+            for (size_t x = a; x < b;) {
+                const size_t e = c.dev ? std::min(b, x + kUploadChunk) : b;
+                stream_copy((char *)c.dst + (x - base), (const char *)c.src + (x - base), e - x);
+                // the non-temporal stores are fenced inside stream_copy, so the
+                // bytes are in memory before the copy engine reads them
+                if (c.dev) {
+                    const cudaError_t ce = cudaMemcpyAsync((char *)c.dev + (x - base), (const char *)c.dst + (x - base),
+                                                           e - x, cudaMemcpyHostToDevice, st);
+                    if (ce != cudaSuccess) err.store((int)ce);
+                }
+                x = e;
+            }
             base += c.bytes;
         }
     };
     if (parts <= 1) {
         run(0);
-        return;
+        return err.load();
     }
     std::vector<std::thread> th;
     th.reserve(parts - 1);
     for (int k = 1; k < parts; ++k) th.emplace_back(run, k);
     run(0);
     for (std::thread &t : th) t.join();
+    return err.load();
 }
 
 // ConvertDepthtoUChar (planesweep.cpp:279-290) per pixel, for the sweep
@@ -131,13 +153,25 @@ struct PlaneSweepImpl {
     DevBuf ref, srcs, H, depths, depth, depth8, labels, best, ws, denoised, tvws, tvu, cx, cy, cz, tvsrc;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int n_views = 0, n_planes = 0, w = 0, h = 0;
+    // Images that the C-ABI setters (the only writers of the host images of a
+    // handle) uploaded while staging them: RunAlgorithm then uploads neither.
+    // `uploaded` marks the end of those copies; the host images are not
+    // rewritten or freed before it.
+    bool ref_dev = false;
+    int srcs_dev = 0, dev_w = 0, dev_h = 0;
+    cudaEvent_t uploaded = nullptr;
     PlaneSweepImpl()
     {
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
+        if (cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming) != cudaSuccess) uploaded = nullptr;
     }
     ~PlaneSweepImpl()
     {
+        if (uploaded) {
+            cudaEventSynchronize(uploaded);
+            cudaEventDestroy(uploaded);
+        }
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
     }
@@ -241,14 +275,18 @@ bool PlaneSweep::RunAlgorithm(int, char **)
     const size_t wsb = mvs_sweep_workspace_bytes(&d);
     if (wsb == 0) return false;
     const size_t lab_n = sweepmode == MVS_SWEEP_PER_VIEW ? n * nimgs : n;
+    // images the C-ABI setters uploaded already (buffers that do not grow keep them)
+    const bool ref_up = I.ref_dev && I.dev_w == w && I.dev_h == h && I.ref.bytes >= n * 4;
+    const bool srcs_up = I.srcs_dev >= nimgs && I.dev_w == w && I.dev_h == h && I.srcs.bytes >= n * 4 * nimgs;
     if (I.ref.ensure(n * 4) || I.srcs.ensure(n * 4 * nimgs) || I.H.ensure((size_t)nimgs * P * 9 * 4) ||
         I.depths.ensure((size_t)P * 4) || I.depth.ensure(n * 4) || I.labels.ensure(lab_n * 4) ||
         I.best.ensure(lab_n * 4) || I.ws.ensure(wsb) || I.depth8.ensure(n))
         return false;
     depthmap8u.reset(w, h);
     cudaStream_t st = 0;
-    if (cudaMemcpyAsync(I.ref.p, HostRef.data(), n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) goto cuda_fail;
-    for (int v = 0; v < nimgs; ++v)
+    if (!ref_up && cudaMemcpyAsync(I.ref.p, HostRef.data(), n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        goto cuda_fail;
+    for (int v = 0; v < nimgs && !srcs_up; ++v)
         if (cudaMemcpyAsync(I.srcs.as<float>() + v * n, HostSrc[v].data(), n * 4, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             goto cuda_fail;
@@ -595,10 +633,25 @@ int mvs_ps_set_reference(mvs_planesweep *ps, const float *img, int32_t w, int32_
 {
     PS_CHECK(ps);
     if (!img || w <= 0 || h <= 0 || !R9 || !t3) return mvs::set_error(MVS_ERR_ARG, "bad reference image");
+    PlaneSweepImpl &I = *ps->ps.impl;
+    // the previous uploads still read the host images (no event: no device,
+    // the images stay on the host for RunAlgorithm)
+    if (I.uploaded) cudaEventSynchronize(I.uploaded);
+    const size_t bytes = sizeof(float) * (size_t)w * h;
     ps->ps.HostRef.reset(w, h);
-    mvs::parallel_copy({{ps->ps.HostRef.data(), img, sizeof(float) * (size_t)w * h}});
     ps->ps.HostRef.R = Matrix3D(R9);
     ps->ps.HostRef.t = Vector3D(t3);
+    I.ref_dev = false;
+    if (w != I.dev_w || h != I.dev_h) I.srcs_dev = 0;
+    // staged and uploaded together (RunAlgorithm's stream); a failed upload
+    // leaves the image to RunAlgorithm
+    const bool up = I.uploaded && I.ref.ensure(bytes) == MVS_OK;
+    const int rc = mvs::parallel_copy({{ps->ps.HostRef.data(), img, bytes, up ? I.ref.p : nullptr}}, 0);
+    if (up && rc == 0 && cudaEventRecord(I.uploaded, 0) == cudaSuccess) {
+        I.ref_dev = true;
+        I.dev_w = w;
+        I.dev_h = h;
+    }
     return MVS_OK;
 }
 
@@ -608,15 +661,26 @@ int mvs_ps_set_sources(mvs_planesweep *ps, const float *imgs, int32_t n, const f
     const int w = (int)ps->ps.HostRef.width(), h = (int)ps->ps.HostRef.height();
     if (w == 0) return mvs::set_error(MVS_ERR_STATE, "set the reference image first");
     if (n < 0 || (n > 0 && (!imgs || !R9s || !t3s))) return mvs::set_error(MVS_ERR_ARG, "bad source images");
+    PlaneSweepImpl &I = *ps->ps.impl;
+    if (I.uploaded) cudaEventSynchronize(I.uploaded);
+    const size_t bytes = sizeof(float) * (size_t)w * h;
+    I.srcs_dev = 0;
+    const bool up = I.uploaded && n > 0 && I.srcs.ensure(bytes * n) == MVS_OK;
     ps->ps.HostSrc.resize(n);
     std::vector<mvs::CopyPiece> pieces;
     for (int v = 0; v < n; ++v) {
         ps->ps.HostSrc[v].reset(w, h);
-        pieces.push_back({ps->ps.HostSrc[v].data(), imgs + (size_t)v * w * h, sizeof(float) * (size_t)w * h});
+        pieces.push_back({ps->ps.HostSrc[v].data(), imgs + (size_t)v * w * h, bytes,
+                          up ? (void *)(I.srcs.as<char>() + bytes * v) : nullptr});
         ps->ps.HostSrc[v].R = Matrix3D(R9s + 9 * v);
         ps->ps.HostSrc[v].t = Vector3D(t3s + 3 * v);
     }
-    mvs::parallel_copy(pieces);
+    const int rc = mvs::parallel_copy(pieces, 0);
+    if (up && rc == 0 && cudaEventRecord(I.uploaded, 0) == cudaSuccess) {
+        I.srcs_dev = n;
+        I.dev_w = w;
+        I.dev_h = h;
+    }
     return MVS_OK;
 }
 

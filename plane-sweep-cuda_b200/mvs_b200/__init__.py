@@ -591,9 +591,10 @@ class FusionVolume:
         self.h = h
 
     def close(self):
-        if getattr(self, "h", None) and self.h.value:
+        # _L is None once the interpreter is tearing the module down
+        if getattr(self, "h", None) and self.h.value and _L is not None:
             _L.mvs_fusion_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -680,9 +681,10 @@ class PlaneSweep:
         self.n_views = 0
 
     def close(self):
-        if getattr(self, "h", None) and self.h.value:
+        # _L is None once the interpreter is tearing the module down
+        if getattr(self, "h", None) and self.h.value and _L is not None:
             _L.mvs_ps_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
