@@ -238,6 +238,35 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
     }
 }
 
+// The NCC of a run of RUN outputs against the reference moments, which are
+// read in groups of four (one 16-byte load each when RUN is a multiple of 4),
+// so at most four of them are live at a time.
+template <int WIN, int MOM, typename F>
+__device__ __forceinline__ void ncc_run(const float *s1, const float *s2, const float *s12, const float *rmrow,
+                                        const float *rsrow, float st, F &&use)
+{
+    using G = Geo<WIN>;
+#pragma unroll
+    for (int j0 = 0; j0 < G::RUN; j0 += 4) {
+        float rm[4], rs[4];
+        if constexpr (G::RUN % 4 == 0) {
+            const float4 a = *reinterpret_cast<const float4 *>(rmrow + j0);
+            const float4 b = *reinterpret_cast<const float4 *>(rsrow + j0);
+            rm[0] = a.x, rm[1] = a.y, rm[2] = a.z, rm[3] = a.w;
+            rs[0] = b.x, rs[1] = b.y, rs[2] = b.z, rs[3] = b.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                rm[i] = j0 + i < G::RUN ? rmrow[j0 + i] : 0.f;
+                rs[i] = j0 + i < G::RUN ? rsrow[j0 + i] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (j0 + i < G::RUN) use(j0 + i, ncc_of<WIN, MOM>(s1[j0 + i], s2[j0 + i], s12[j0 + i], rm[i], rs[i], st));
+    }
+}
+
 // Shared-memory layout of one CTA.
 struct __align__(16) Smem {
     float Wt[RHMAX][RWMAX];        // warped region (reference region at start)
@@ -581,14 +610,12 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             __syncthreads();
             pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
             __syncthreads();
-            float s1[G::RUN], s2[G::RUN], s12[G::RUN], rm[G::RUN], rs[G::RUN];
+            float s1[G::RUN], s2[G::RUN], s12[G::RUN];
             row_sums<WIN, MOM>(S.CS[0], s1);
             row_sums<WIN, MOM>(S.CS[1], s2);
             row_sums<WIN, MOM>(S.CS[2], s12);
-            load_run<G::RUN, G::RUN>(A.RM[ly] + lx, rm);
-            load_run<G::RUN, G::RUN>(A.RS[ly] + lx, rs);
-#pragma unroll
-            for (int j = 0; j < G::RUN; ++j) acc[j] += ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
+            ncc_run<WIN, MOM>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh,
+                              [&](int j, float c) { acc[j] += c; });
         }
         uint16_t cb[G::RUN];
 #pragma unroll
@@ -693,20 +720,16 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         __syncthreads();   // Wt and the next homography visible; pass B of the previous plane done with CS
         pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
         __syncthreads();
-        float s1[G::RUN], s2[G::RUN], s12[G::RUN], rm[G::RUN], rs[G::RUN];
+        float s1[G::RUN], s2[G::RUN], s12[G::RUN];
         row_sums<WIN, MOM>(S.CS[0], s1);
         row_sums<WIN, MOM>(S.CS[1], s2);
         row_sums<WIN, MOM>(S.CS[2], s12);
-        load_run<G::RUN, G::RUN>(A.RM[ly] + lx, rm);
-        load_run<G::RUN, G::RUN>(A.RS[ly] + lx, rs);
-#pragma unroll
-        for (int j = 0; j < G::RUN; ++j) {
-            const float c = ncc_of<WIN, MOM>(s1[j], s2[j], s12[j], rm[j], rs[j], a.stdthresh);
+        ncc_run<WIN, MOM>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh, [&](int j, float c) {
             if (c > best[j]) {
                 best[j] = c;
                 lab[j] = p;
             }
-        }
+        });
     }
     // results: (ncc bits << 32) | ~plane, so that a 64-bit max keeps the
     // largest NCC and, among equal NCCs, the earliest plane.

@@ -75,3 +75,44 @@ def test_errors_are_reported_not_raised_on_device(cuda):
         ps.RunAlgorithm()            # no images yet
     with pytest.raises(M.MvsError):
         ps.setWindowSize(4)          # even window
+
+
+def test_images_set_again_between_runs(cuda, golden):
+    """The image setters upload while they stage and RunAlgorithm skips those
+    uploads: new sources, a repeated run and a new frame size on one handle give
+    the depthmaps of fresh handles (never a stale device image)."""
+    g = golden("sweep_inverse_w5")
+    ps = make_ps(g, True)
+    ps.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
+    ps.RunAlgorithm()   # nothing set again: the same images
+    np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
+    # other sources (the list reversed), then the originals again
+    g2 = dict(g)
+    g2["srcs"], g2["Rsrc"], g2["tsrc"] = g["srcs"][::-1], g["Rsrc"][::-1], g["tsrc"][::-1]
+    ps.set_sources(list(g2["srcs"]), list(g2["Rsrc"]), list(g2["tsrc"]))
+    ps.RunAlgorithm()
+    fresh = make_ps(g2, True)
+    fresh.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), fresh.getDepthmap())
+    ps.set_sources(list(g["srcs"]), list(g["Rsrc"]), list(g["tsrc"]))
+    ps.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
+    # a smaller frame (the top-left crop) on the same handle
+    h, w = g["ref"].shape
+    g3 = dict(g)
+    g3["ref"] = np.ascontiguousarray(g["ref"][: h - 8, : w - 16])
+    g3["srcs"] = np.ascontiguousarray(np.asarray(g["srcs"])[:, : h - 8, : w - 16])
+    ps.set_reference(g3["ref"], g3["Rref"], g3["tref"])
+    ps.set_sources(list(g3["srcs"]), list(g3["Rsrc"]), list(g3["tsrc"]))
+    ps.RunAlgorithm()
+    fresh3 = make_ps(g3, True)
+    fresh3.RunAlgorithm()
+    assert ps.getDepthmap().shape == (h - 8, w - 16)
+    np.testing.assert_array_equal(ps.getDepthmap(), fresh3.getDepthmap())
+    # the reference set again alone, after the sources
+    ps.set_reference(g3["ref"], g3["Rref"], g3["tref"])
+    ps.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), fresh3.getDepthmap())
+    for p in (ps, fresh, fresh3):
+        p.close()

@@ -7,7 +7,13 @@ winner-take-all depth (plain) and once from the network's prediction (warm),
 both linearised at the winner-take-all depth so they minimise the same
 energy.  The warm run must end at an energy no higher than the plain run's
 (0.5% slack per frame), get below the plain run's final energy in a fraction
-of its iterations, and take less device time including the network."""
+of its iterations, and take less device time including the network.
+
+The speed claim is made at equal energy: the warm run reaches the plain run's
+final energy at least 3x sooner (network included).  Times to the tolerance
+compare runs that stop at different energies -- a plain run can stop on a
+plateau far above the warm run's energy (seed 910001: 120 iterations, 81%
+higher) -- so there the warm runs need only take less time in total."""
 import numpy as np
 import pytest
 
@@ -29,5 +35,8 @@ def test_warm_start_beats_plain_tgv2(cuda):
     reach = np.median([r["warm_iters_to_plain_energy"] for r in rows])
     plain_it = np.median([r["plain_iters"] for r in rows])
     assert reach * 3 <= plain_it, (reach, plain_it)
-    speedup = np.mean([r["plain_ms"] for r in rows]) / np.mean([r["warm_ms"] for r in rows])
-    assert speedup >= 1.5, speedup
+    plain_ms = np.mean([r["plain_ms"] for r in rows])
+    to_plain_energy = plain_ms / np.mean([r["warm_ms_to_plain_energy"] for r in rows])
+    assert to_plain_energy >= 3.0, to_plain_energy
+    to_tolerance = plain_ms / np.mean([r["warm_ms"] for r in rows])
+    assert to_tolerance > 1.0, to_tolerance
