@@ -161,8 +161,12 @@ def bf16_round(x):
     return (u.astype(np.uint32) << 16).view(np.float32)
 
 
-def test_aggregated_bf16_wta_vs_fp64_oracle(cuda):
-    fr, planes, win = scenes.config_tiny(seed=5, width=96, height=64, n_src=3, n_planes=24, win=7)
+@pytest.mark.parametrize("win,width,height", [(7, 96, 64), (3, 70, 45), (5, 131, 40), (11, 120, 70), (15, 77, 52)])
+def test_aggregated_bf16_wta_vs_fp64_oracle(cuda, win, width, height):
+    """Every tile layout of the aggregated kernel: 64-wide tiles with 8-output
+    runs (3x3 to 9x9, regions of 66 to 72 columns) and 56-wide tiles with
+    7-output runs (11x11 and up); frame sizes that do not divide the tiles."""
+    fr, planes, win = scenes.config_tiny(seed=5, width=width, height=height, n_src=3, n_planes=24, win=win)
     poses = [(c.R, c.t) for c in fr.src_cams]
     K1 = fr.ref_cam.K_1based
     H64 = po.homographies(K1, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f64")
