@@ -315,7 +315,10 @@ int mvs_ps_tgv_denoise_from_sparse(mvs_planesweep *ps, const float *h_sparse, in
  * h_u_init (start = 2) or from 1 (start = 0), with an energy tolerance. */
 int mvs_ps_tgv_ext(mvs_planesweep *ps, const mvs_tgv2_params *params, int32_t start, const float *h_u_init,
                    int32_t *iters_out, double *energy_out);
-/* Getters (planesweep.h:287-437).  Image getters copy width*height values. */
+/* Getters (planesweep.h:287-437).  Image getters copy width*height values of
+ * the current reference frame (mvs_ps_get_size); a result of a frame of
+ * another size (the reference was set again since) is refused with
+ * MVS_ERR_STATE. */
 int mvs_ps_get_size(mvs_planesweep *ps, int32_t *width, int32_t *height);
 int mvs_ps_get_depthmap(mvs_planesweep *ps, float *out);
 int mvs_ps_get_depthmap8u(mvs_planesweep *ps, uint8_t *out);
@@ -325,7 +328,8 @@ int mvs_ps_get_depthmap_tgv(mvs_planesweep *ps, float *out);
 int mvs_ps_get_depthmap8u_tgv(mvs_planesweep *ps, uint8_t *out);
 /* getDepthmapDenoisedPtr: device pointer, overwritten by each CudaDenoise. */
 int mvs_ps_get_depthmap_denoised_ptr(mvs_planesweep *ps, float **d_ptr);
-/* Per-view labels / best NCC of the last sweep (n_views*H*W), extension. */
+/* Per-view labels / best NCC of the last sweep (n_views*H*W, n_views the
+ * views that sweep used: at most the number of sources), extension. */
 int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out);
 int mvs_ps_get_view_best(mvs_planesweep *ps, float *out);
 int mvs_ps_get_3d_coordinates(mvs_planesweep *ps, float *X, float *Y, float *Z); /* get3Dcoordinates */

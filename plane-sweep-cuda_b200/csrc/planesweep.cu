@@ -827,39 +827,55 @@ int mvs_ps_get_size(mvs_planesweep *ps, int32_t *w, int32_t *h)
     return MVS_OK;
 }
 
-static int copy_image(const CamImage<float> *img, float *out)
+// The image getters copy width * height values of the current reference
+// frame (mvs_ps_get_size): a result of a frame of another size (the reference
+// was set again since) is refused rather than copied past the caller's buffer.
+static int frame_check(const mvs_planesweep *ps, size_t w, size_t h, const char *what)
 {
-    if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
-    if (!img || img->empty()) return mvs::set_error(MVS_ERR_STATE, "no such depthmap yet");
-    memcpy(out, img->data(), sizeof(float) * img->elements());
+    const size_t W = ps->ps.HostRef.width(), H = ps->ps.HostRef.height();
+    if (w != W || h != H)
+        return mvs::set_error(MVS_ERR_STATE, "the %s is of a %zux%zu frame, the reference is now %zux%zu: run again",
+                              what, w, h, W, H);
     return MVS_OK;
 }
 
-static int copy_image8(const CamImage<uchar> *img, uint8_t *out)
+extern "C++" {
+template <typename T>
+static int copy_image(const mvs_planesweep *ps, const CamImage<T> *img, T *out)
 {
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
     if (!img || img->empty()) return mvs::set_error(MVS_ERR_STATE, "no such depthmap yet");
-    memcpy(out, img->data(), img->elements());
+    if (int rc = frame_check(ps, img->width(), img->height(), "depthmap")) return rc;
+    memcpy(out, img->data(), sizeof(T) * img->elements());
     return MVS_OK;
 }
+}
 
-int mvs_ps_get_depthmap(mvs_planesweep *ps, float *out) { PS_CHECK(ps); return copy_image(ps->ps.getDepthmap(), out); }
-int mvs_ps_get_depthmap8u(mvs_planesweep *ps, uint8_t *out) { PS_CHECK(ps); return copy_image8(ps->ps.getDepthmap8u(), out); }
+int mvs_ps_get_depthmap(mvs_planesweep *ps, float *out) { PS_CHECK(ps); return copy_image(ps, ps->ps.getDepthmap(), out); }
+int mvs_ps_get_depthmap8u(mvs_planesweep *ps, uint8_t *out)
+{
+    PS_CHECK(ps);
+    return copy_image(ps, ps->ps.getDepthmap8u(), out);
+}
 int mvs_ps_get_depthmap_denoised(mvs_planesweep *ps, float *out)
 {
     PS_CHECK(ps);
-    return copy_image(ps->ps.getDepthmapDenoised(), out);
+    return copy_image(ps, ps->ps.getDepthmapDenoised(), out);
 }
 int mvs_ps_get_depthmap8u_denoised(mvs_planesweep *ps, uint8_t *out)
 {
     PS_CHECK(ps);
-    return copy_image8(ps->ps.getDepthmap8uDenoised(), out);
+    return copy_image(ps, ps->ps.getDepthmap8uDenoised(), out);
 }
-int mvs_ps_get_depthmap_tgv(mvs_planesweep *ps, float *out) { PS_CHECK(ps); return copy_image(ps->ps.getDepthmapTGV(), out); }
+int mvs_ps_get_depthmap_tgv(mvs_planesweep *ps, float *out)
+{
+    PS_CHECK(ps);
+    return copy_image(ps, ps->ps.getDepthmapTGV(), out);
+}
 int mvs_ps_get_depthmap8u_tgv(mvs_planesweep *ps, uint8_t *out)
 {
     PS_CHECK(ps);
-    return copy_image8(ps->ps.getDepthmap8uTGV(), out);
+    return copy_image(ps, ps->ps.getDepthmap8uTGV(), out);
 }
 
 int mvs_ps_get_depthmap_denoised_ptr(mvs_planesweep *ps, float **d_ptr)
@@ -876,6 +892,8 @@ int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out)
     const std::vector<int32_t> &v = ps->ps.getViewLabels();
     if (v.empty()) return mvs::set_error(MVS_ERR_STATE, "no sweep result");
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
+    const CamImage<float> *d = ps->ps.getDepthmap();   // of the same sweep
+    if (int rc = frame_check(ps, d->width(), d->height(), "sweep result")) return rc;
     memcpy(out, v.data(), v.size() * 4);
     return MVS_OK;
 }
@@ -886,6 +904,8 @@ int mvs_ps_get_view_best(mvs_planesweep *ps, float *out)
     const std::vector<float> &v = ps->ps.getViewBest();
     if (v.empty()) return mvs::set_error(MVS_ERR_STATE, "no sweep result");
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
+    const CamImage<float> *d = ps->ps.getDepthmap();
+    if (int rc = frame_check(ps, d->width(), d->height(), "sweep result")) return rc;
     memcpy(out, v.data(), v.size() * 4);
     return MVS_OK;
 }
@@ -896,6 +916,7 @@ int mvs_ps_get_3d_coordinates(mvs_planesweep *ps, float *X, float *Y, float *Z)
     CamImage<float> *x, *y, *z;
     ps->ps.get3Dcoordinates(x, y, z);
     if (!x) return MVS_ERR_STATE;
+    if (int rc = frame_check(ps, x->width(), x->height(), "point map")) return rc;
     if (X) memcpy(X, x->data(), x->elements() * 4);
     if (Y) memcpy(Y, y->data(), y->elements() * 4);
     if (Z) memcpy(Z, z->data(), z->elements() * 4);

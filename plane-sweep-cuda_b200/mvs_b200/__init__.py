@@ -757,7 +757,8 @@ class PlaneSweep:
         return it.value, e.value
 
     def _img(self, name, dtype=np.float32):
-        out = np.zeros(self.shape, dtype)
+        # every element is written: the library refuses a map of another size
+        out = np.empty(self.shape, dtype)
         ptr = out.ctypes.data_as(_F if dtype == np.float32 else _U8)
         check(getattr(_L, f"mvs_ps_get_{name}")(self.h, ptr))
         return out

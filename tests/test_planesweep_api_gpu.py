@@ -116,3 +116,19 @@ def test_images_set_again_between_runs(cuda, golden):
     np.testing.assert_array_equal(ps.getDepthmap(), fresh3.getDepthmap())
     for p in (ps, fresh, fresh3):
         p.close()
+
+
+def test_getters_refuse_a_map_of_another_frame_size(cuda, golden):
+    """After the reference is set again at another size, the last run's maps no
+    longer fit the getters' width*height contract: they are refused, not copied."""
+    g = golden("sweep_inverse_w5")
+    ps = make_ps(g, True)
+    ps.RunAlgorithm()
+    h, w = g["ref"].shape
+    ps.set_reference(np.ascontiguousarray(g["ref"][: h // 2, : w // 2]), g["Rref"], g["tref"])
+    for get in (ps.getDepthmap, ps.getDepthmap8u, ps.getViewLabels, ps.getViewBest):
+        with pytest.raises(M.MvsError):
+            get()
+    ps.set_reference(g["ref"], g["Rref"], g["tref"])   # the run's size again
+    np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
+    ps.close()
