@@ -14,8 +14,10 @@
 //       kernels.cu:66-82: strictly greater wins, so ties keep the earlier
 //       plane and NCC <= 0 never wins).
 // This replaces the reference's 12 full-image launches per plane and view
-// (planesweep.cpp:205-249) with two barriers per plane and no HBM traffic
-// except the source gathers (L1/L2 resident) and one result write per pixel.
+// (planesweep.cpp:205-249) with two barriers per plane and view and no HBM
+// traffic except the source gathers (L1/L2 resident) and the results (one
+// word per pixel; in the aggregated mode also the BF16 cost per pixel and
+// plane, written as 16-byte runs).
 //
 // Moments:
 //   MVS_MOMENTS_REFERENCE   the reference's box means (column pass then row
