@@ -10,6 +10,7 @@ import pytest
 
 import pyoracle as po
 import mvs_b200 as M
+from mvs_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -132,3 +133,57 @@ def test_getters_refuse_a_map_of_another_frame_size(cuda, golden):
     ps.set_reference(g["ref"], g["Rref"], g["tref"])   # the run's size again
     np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
     ps.close()
+
+
+def _rel_like_the_handle(Rref, tref, Rsrc, tsrc):
+    """RunAlgorithm's FP64 relative pose from the float poses: Rsrc * Rref^-1
+    with the adjugate / determinant inverse, in the same operation order."""
+    m = [float(x) for x in np.asarray(Rref, np.float32).reshape(9)]
+    rs = [float(x) for x in np.asarray(Rsrc, np.float32).reshape(9)]
+    tr = [float(x) for x in np.asarray(tref, np.float32).reshape(3)]
+    ts = [float(x) for x in np.asarray(tsrc, np.float32).reshape(3)]
+    det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6])
+    inv = [(m[4] * m[8] - m[5] * m[7]) / det, (m[2] * m[7] - m[1] * m[8]) / det, (m[1] * m[5] - m[2] * m[4]) / det,
+           (m[5] * m[6] - m[3] * m[8]) / det, (m[0] * m[8] - m[2] * m[6]) / det, (m[2] * m[3] - m[0] * m[5]) / det,
+           (m[3] * m[7] - m[4] * m[6]) / det, (m[1] * m[6] - m[0] * m[7]) / det, (m[0] * m[4] - m[1] * m[3]) / det]
+    Ro = [rs[3 * r] * inv[c] + rs[3 * r + 1] * inv[3 + c] + rs[3 * r + 2] * inv[6 + c] for r in range(3) for c in range(3)]
+    to = [ts[r] - (Ro[3 * r] * tr[0] + Ro[3 * r + 1] * tr[1] + Ro[3 * r + 2] * tr[2]) for r in range(3)]
+    return np.array(Ro).reshape(3, 3), np.array(to)
+
+
+def test_full_size_frame_through_the_handle_equals_device_entry_point(cuda):
+    """640x480, 8 views (11 MB of images: staged by several threads and uploaded
+    MB by MB as they are copied): the handle's depthmap is bit-identical to
+    mvs_sweep's on device copies of the same images and homographies."""
+    import torch
+    fr, planes, win = scenes.config_full(seed=6)
+    planes = planes[::4].copy()          # 64 planes: the upload path does not depend on them
+    V = len(fr.srcs)
+    K1 = np.float32(fr.ref_cam.K_1based)
+    ps = M.PlaneSweep()
+    ps.setK(K1)
+    ps.setPlaneDepths(planes)
+    ps.setWindowSize(win)
+    ps.setNumberofImages(V)
+    ps.setZ(0.4, 8.0)
+    ps.setSweepOptions(M.MOMENTS_COMPENSATED, M.SWEEP_AGGREGATED, True)
+    Rs = np.stack([c.R for c in fr.src_cams]).astype(np.float32)
+    ts = np.stack([c.t for c in fr.src_cams]).astype(np.float32)
+    ps.set_reference(fr.ref, fr.ref_cam.R, fr.ref_cam.t)
+    ps.set_sources(np.stack(fr.srcs), Rs, ts)
+    ps.RunAlgorithm()
+    got = ps.getDepthmap()
+    ps.close()
+    h, w = fr.ref.shape
+    desc = M.sweep_desc(w, h, V, len(planes), win, M.MOMENTS_COMPENSATED, M.SWEEP_AGGREGATED, 1e-4, 0.5, 8.0)
+    d_ref = torch.from_numpy(np.ascontiguousarray(fr.ref, np.float32)).to(cuda)
+    d_srcs = torch.from_numpy(np.ascontiguousarray(np.stack(fr.srcs), np.float32)).to(cuda)
+    d_depths = torch.from_numpy(np.ascontiguousarray(planes, np.float32)).to(cuda)
+    H = torch.empty((V, len(planes), 9), dtype=torch.float32, device=cuda)
+    rel = [_rel_like_the_handle(fr.ref_cam.R, fr.ref_cam.t, Rs[v], ts[v]) for v in range(V)]
+    M.sweep_homographies(desc, np.float64(K1), rel, d_depths, H)
+    depth = torch.empty((h, w), dtype=torch.float32, device=cuda)
+    ws = torch.empty(M.sweep_workspace_bytes(desc), dtype=torch.uint8, device=cuda)
+    M.sweep(desc, d_ref, d_srcs, H, d_depths, depth, workspace=ws)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(got, depth.cpu().numpy())
