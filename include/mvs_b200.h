@@ -118,11 +118,16 @@ int mvs_sweep(const mvs_sweep_desc *desc, const float *d_ref, const float *d_src
  * real-time loops that cannot take cudaMalloc's latency and implicit
  * synchronisation.  The sweep's scratch (one 64-bit word per pixel and view,
  * or per pixel in the aggregated mode) lives in a fixed device array of
- * mvs_sweep_noalloc_scratch_bytes() = 32 MiB inside the library, which every
- * GPU that loads the library holds until the process exits; a larger sweep
- * is rejected with MVS_ERR_ARG.  Nothing is allocated: the first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call outside any stream capture.  All calls share the one array,
+ * mvs_sweep_noalloc_scratch_bytes() = 32 MiB inside the library, which a GPU
+ * holds from the first call on it until the process exits; a larger sweep
+ * is rejected with MVS_ERR_ARG.  The call itself allocates nothing (no
+ * cudaMalloc, no cudaFree).  The array is reserved when CUDA loads the module
+ * that holds it, which under CUDA's default lazy module loading happens at the
+ * first call on each device: that call looks up the array's device address
+ * (cudaGetSymbolAddress), which loads the module and reserves the 32 MiB then.
+ * So make that first call at start-up (a small frame will do) and outside any
+ * stream capture.  Every call looks the address up again for the current
+ * device and context.  All calls share the one array,
  * which keeps the last call's contents: calls that can overlap on the GPU
  * (other streams, other host threads) race and must be serialised by the
  * caller.  Arguments and outputs as mvs_sweep. */

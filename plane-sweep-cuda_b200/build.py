@@ -22,7 +22,9 @@ CSRC = PKG / "csrc"
 OUT = PKG / "mvs_b200" / "libmvs_b200.so"
 BUILD = PKG / "_build"
 ORACLE = ROOT / "oracle"
-REFERENCE_SRC = pathlib.Path("/root/reference/src")
+# The reference's source tree (its src/ folder), used only to build the test
+# oracles; set MVS_REFERENCE_SRC to point elsewhere.  Absent -> only the C oracle.
+REFERENCE_SRC = pathlib.Path(os.environ.get("MVS_REFERENCE_SRC", "/root/reference/src"))
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -80,7 +82,7 @@ def build_oracle(verbose: bool = False) -> None:
     targets = ["oracle"]
     if (REFERENCE_SRC / "kernels.cu").exists():
         targets += ["ref", "ref_gpu"]
-    r = subprocess.run(["make", "-C", str(ORACLE), *targets], capture_output=True, text=True)
+    r = subprocess.run(["make", "-C", str(ORACLE), f"REF={REFERENCE_SRC}", *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
     if verbose:

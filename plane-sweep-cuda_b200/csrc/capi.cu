@@ -30,7 +30,7 @@ int check_launch(const char *what)
     return MVS_OK;
 }
 
-static void clear_error() { g_err[0] = 0; }
+void clear_error() { g_err[0] = 0; }
 
 // sweep.cu
 int sweep_pick_chunks(int win, int w, int h, int V, int P, int mode);
@@ -161,7 +161,9 @@ int mvs_set_device(int device)
 
 // ---- sweep ----------------------------------------------------------------------------
 
-static int check_sweep_desc(const mvs_sweep_desc *d)
+}  // extern "C"
+
+int mvs::check_sweep_desc(const mvs_sweep_desc *d)
 {
     if (!d) return set_error(MVS_ERR_ARG, "null sweep descriptor");
     if (d->width <= 0 || d->height <= 0 || d->n_views <= 0 || d->n_planes <= 0)
@@ -181,6 +183,8 @@ static int check_sweep_desc(const mvs_sweep_desc *d)
         return set_error(MVS_ERR_ARG, "aggregated mode: at most 65535 planes (%d)", d->n_planes);
     return MVS_OK;
 }
+
+extern "C" {
 
 size_t mvs_sweep_workspace_bytes(const mvs_sweep_desc *d)
 {

@@ -19,6 +19,9 @@ constexpr int kMapCamFloats = 21;  // per fusion depthmap: K[9] R[9] t[3]
 // Last-error bookkeeping shared by every entry point (defined in capi.cu).
 int set_error(int code, const char *fmt, ...);
 int check_launch(const char *what);
+void clear_error();
+// Validates a sweep descriptor; MVS_OK or MVS_ERR_ARG with the message set.
+int check_sweep_desc(const mvs_sweep_desc *d);
 
 #define MVS_TRY_CUDA(expr)                                                              \
     do {                                                                                \

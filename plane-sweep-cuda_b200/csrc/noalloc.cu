@@ -9,13 +9,16 @@
 // needs beyond those -- the per-pixel best-match words that the sweep kernel
 // and its epilogue exchange -- lives in `g_sweep_scratch` below.
 //
-// The array is a file-scope __device__ variable: every GPU that loads the
-// library holds its kNoAllocScratchBytes until the process exits.  Host code
-// must not pass the array's name to a kernel (on the host that name is a
-// stand-in, not a device address), so the device address is looked up once per
-// device with cudaGetSymbolAddress and cached.
-#include <mutex>
-
+// The array is a file-scope __device__ variable of this file's CUDA module.
+// CUDA loads a module lazily (the default since CUDA 12.2): the first time
+// host code touches it on a device, here the first cudaGetSymbolAddress of a
+// call on that device.  That load reserves the array's 32 MiB on the device,
+// which then holds it until the process exits.  Host code must not pass the
+// array's name to a kernel (on the host that name is a stand-in, not a device
+// address), so every call looks the device address up with
+// cudaGetSymbolAddress for the current device and context; once the module is
+// loaded the lookup is cheap, and it stays right after a device reset or when
+// a caller's own context is current.
 #include "common.cuh"
 
 namespace mvs {
@@ -32,32 +35,6 @@ size_t sweep_scratch_bytes(const mvs_sweep_desc *d);
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
 static __device__ __align__(256) unsigned long long g_sweep_scratch[kNoAllocScratchBytes / 8];
 
-namespace {
-
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-void *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_sweep_scratch on the current device (looked up on the
-// first call for that device, with that device current).
-int scratch_address(void **out)
-{
-    int dev = 0;
-    MVS_TRY_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(MVS_ERR_ARG, "device %d out of range", dev);
-    std::lock_guard<std::mutex> g(g_lock);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
-        if (e != cudaSuccess)
-            return set_error(MVS_ERR_CUDA, "cudaGetSymbolAddress(sweep scratch): %s", cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
-    return MVS_OK;
-}
-
-}  // namespace
 }  // namespace mvs
 
 extern "C" {
@@ -68,7 +45,8 @@ int mvs_sweep_noalloc(const mvs_sweep_desc *d, const float *ref, const float *sr
                       const float *depths, float *depth, int32_t *labels, float *best, uint16_t *cost, void *stream)
 {
     using namespace mvs;
-    if (mvs_sweep_workspace_bytes(d) == 0) return MVS_ERR_ARG;   // validates d
+    clear_error();
+    if (int rc = check_sweep_desc(d)) return rc;
     // only the winner words: the fixed array holds no 2x2 source neighbourhoods
     // (the kernel then gathers the four samples itself)
     const size_t need = sweep_scratch_bytes(d);
@@ -80,7 +58,9 @@ int mvs_sweep_noalloc(const mvs_sweep_desc *d, const float *ref, const float *sr
     if (!ref || !srcs || !H || !depths || !depth) return set_error(MVS_ERR_ARG, "null input/output pointer");
     if (d->mode == MVS_SWEEP_PER_VIEW && cost) return set_error(MVS_ERR_ARG, "cost volume is an aggregated-mode output");
     void *scratch = nullptr;
-    if (int rc = scratch_address(&scratch)) return rc;
+    const cudaError_t e = cudaGetSymbolAddress(&scratch, g_sweep_scratch);
+    if (e != cudaSuccess)
+        return set_error(MVS_ERR_CUDA, "cudaGetSymbolAddress(sweep scratch): %s", cudaGetErrorString(e));
     const int chunks = sweep_pick_chunks(d->window, d->width, d->height, d->n_views, d->n_planes, d->mode);
     return sweep_launch(d, ref, srcs, H, depths, depth, labels, best, cost, (unsigned long long *)scratch, chunks,
                         stream, nullptr);

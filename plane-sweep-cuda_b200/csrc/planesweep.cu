@@ -378,13 +378,20 @@ cuda_fail:
     return false;
 }
 
+// The per-view results are copied back on the first request after a sweep.  A
+// failed copy leaves the vector empty (nothing stale is cached) with the CUDA
+// error as the last error message.
 const std::vector<int32_t> &PlaneSweep::getViewLabels()
 {
     PlaneSweepImpl &I = *impl;
     if (viewlabels.empty() && depthavailable) {
         const size_t m = (size_t)I.w * I.h * (sweepmode == MVS_SWEEP_PER_VIEW ? I.n_views : 1);
         viewlabels.resize(m);
-        cudaMemcpy(viewlabels.data(), I.labels.p, m * 4, cudaMemcpyDeviceToHost);
+        const cudaError_t e = cudaMemcpy(viewlabels.data(), I.labels.p, m * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            viewlabels.clear();
+            mvs::set_error(MVS_ERR_CUDA, "getViewLabels: %s", cudaGetErrorString(e));
+        }
     }
     return viewlabels;
 }
@@ -395,7 +402,11 @@ const std::vector<float> &PlaneSweep::getViewBest()
     if (viewbest.empty() && depthavailable) {
         const size_t m = (size_t)I.w * I.h * (sweepmode == MVS_SWEEP_PER_VIEW ? I.n_views : 1);
         viewbest.resize(m);
-        cudaMemcpy(viewbest.data(), I.best.p, m * 4, cudaMemcpyDeviceToHost);
+        const cudaError_t e = cudaMemcpy(viewbest.data(), I.best.p, m * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            viewbest.clear();
+            mvs::set_error(MVS_ERR_CUDA, "getViewBest: %s", cudaGetErrorString(e));
+        }
     }
     return viewbest;
 }
@@ -889,8 +900,10 @@ int mvs_ps_get_depthmap_denoised_ptr(mvs_planesweep *ps, float **d_ptr)
 int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out)
 {
     PS_CHECK(ps);
+    mvs::clear_error();
     const std::vector<int32_t> &v = ps->ps.getViewLabels();
-    if (v.empty()) return mvs::set_error(MVS_ERR_STATE, "no sweep result");
+    if (v.empty())   // no sweep yet, or the copy back failed (its CUDA error is set)
+        return mvs_last_error()[0] ? MVS_ERR_CUDA : mvs::set_error(MVS_ERR_STATE, "no sweep result");
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
     const CamImage<float> *d = ps->ps.getDepthmap();   // of the same sweep
     if (int rc = frame_check(ps, d->width(), d->height(), "sweep result")) return rc;
@@ -901,8 +914,10 @@ int mvs_ps_get_view_labels(mvs_planesweep *ps, int32_t *out)
 int mvs_ps_get_view_best(mvs_planesweep *ps, float *out)
 {
     PS_CHECK(ps);
+    mvs::clear_error();
     const std::vector<float> &v = ps->ps.getViewBest();
-    if (v.empty()) return mvs::set_error(MVS_ERR_STATE, "no sweep result");
+    if (v.empty())   // no sweep yet, or the copy back failed (its CUDA error is set)
+        return mvs_last_error()[0] ? MVS_ERR_CUDA : mvs::set_error(MVS_ERR_STATE, "no sweep result");
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
     const CamImage<float> *d = ps->ps.getDepthmap();
     if (int rc = frame_check(ps, d->width(), d->height(), "sweep result")) return rc;

@@ -1,8 +1,9 @@
 """Python binding of libmvs_b200 (ctypes over the C ABI of include/mvs_b200.h).
 
-The compute path is the CUDA library only: importing this package loads
+The compute path is the CUDA library only: the first call into it opens
 ``libmvs_b200.so`` and raises ``ImportError`` if it is missing or cannot be
-loaded -- there is no CPU fallback.  Device memory for the device-pointer entry
+loaded -- there is no CPU fallback.  The pure-host modules of the package
+(``scenes``, ``dist``, ``hostmath``) can be imported without opening it.  Device memory for the device-pointer entry
 points is handled with torch tensors (plumbing only; no torch math runs on the
 product path).
 
@@ -38,12 +39,46 @@ class MvsError(RuntimeError):
         self.code = code
 
 
-if not LIB_PATH.exists():
-    raise ImportError(f"{LIB_PATH} is missing: build it with `python plane-sweep-cuda_b200/build.py`")
-try:
-    _L = C.CDLL(str(LIB_PATH))
-except OSError as e:  # pragma: no cover - depends on the box
-    raise ImportError(f"cannot load {LIB_PATH}: {e}") from e
+class _Library:
+    """libmvs_b200.so, opened on the first call into it.
+
+    Signatures declared with ``_sig`` are bound when the library opens.  A
+    missing or unloadable library raises ``ImportError`` at that first call:
+    there is no fallback."""
+
+    def __init__(self):
+        self._cdll = None
+        self._sigs = []
+
+    def declare(self, name, res, args):
+        self._sigs.append((name, res, list(args)))
+        if self._cdll is not None:
+            self._bind(self._cdll, name, res, args)
+
+    @staticmethod
+    def _bind(cdll, name, res, args):
+        f = getattr(cdll, name)
+        f.restype = res
+        f.argtypes = list(args)
+
+    def load(self):
+        if self._cdll is None:
+            if not LIB_PATH.exists():
+                raise ImportError(f"{LIB_PATH} is missing: build it with `python plane-sweep-cuda_b200/build.py`")
+            try:
+                cdll = C.CDLL(str(LIB_PATH))
+            except OSError as e:  # pragma: no cover - depends on the box
+                raise ImportError(f"cannot load {LIB_PATH}: {e}") from e
+            for name, res, args in self._sigs:
+                self._bind(cdll, name, res, args)
+            self._cdll = cdll
+        return self._cdll
+
+    def __getattr__(self, name):
+        return getattr(self.load(), name)
+
+
+_L = _Library()
 
 _F = C.POINTER(C.c_float)
 _D = C.POINTER(C.c_double)
@@ -91,10 +126,7 @@ class BatchTuning(C.Structure):
 
 
 def _sig(name, res, *args):
-    f = getattr(_L, name)
-    f.restype = res
-    f.argtypes = list(args)
-    return f
+    _L.declare(name, res, args)
 
 
 _sig("mvs_last_error", C.c_char_p)
@@ -194,7 +226,8 @@ _sig("mvs_ps_get_last_kernel_ms", C.c_int, _VP, _F)
 
 
 def lib():
-    return _L
+    """The opened ctypes library (opens it on the first call)."""
+    return _L.load()
 
 
 def check(rc):
@@ -446,7 +479,7 @@ class Batch:
         self.n = len(frames)
 
     def close(self):
-        if getattr(self, "_h", None) and _L is not None:
+        if getattr(self, "_h", None) and _L._cdll is not None:
             _L.mvs_batch_destroy(self._h)
         self._h = None
 
@@ -493,7 +526,7 @@ class Unet:
         self._h = h
 
     def close(self):
-        if getattr(self, "_h", None) and _L is not None:
+        if getattr(self, "_h", None) and _L._cdll is not None:
             _L.mvs_unet_destroy(self._h)
         self._h = None
 

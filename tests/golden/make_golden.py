@@ -11,6 +11,7 @@ across machines.
 """
 from __future__ import annotations
 
+import os
 import pathlib
 import sys
 
@@ -23,6 +24,9 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 import pyoracle as po  # noqa: E402
 from mvs_b200 import scenes  # noqa: E402
+
+# The reference's src/ folder (its sample frames); MVS_REFERENCE_SRC overrides the default.
+REFERENCE_SRC = pathlib.Path(os.environ.get("MVS_REFERENCE_SRC", "/root/reference/src"))
 
 
 def frame_arrays(fr):
@@ -156,7 +160,7 @@ def real_frame_case(name, n_src=4, factor=4, n_planes=64, win=5, znear=0.1, zfar
     Outputs of the reference's own kernels: the sweep with its float plane
     loop, the TV-L1 denoise of that depthmap, and TGV2 from it."""
     from PIL import Image
-    src_dir = pathlib.Path("/root/reference/src/PlaneSweep")
+    src_dir = REFERENCE_SRC / "PlaneSweep"
     lines = (src_dir / "Calibration.txt").read_text().splitlines()
     fx, fy, cx, cy, sk = (float(x) for x in lines[0].split())
     W0, H0 = 640, 480

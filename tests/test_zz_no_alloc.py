@@ -3,7 +3,7 @@
 It serves callers that cannot allocate device memory while they run (plugin
 hosts that fix a library's memory at start-up, real-time loops): its scratch
 is a fixed array inside the library.  Checked against mvs_sweep with a caller
-workspace, on two calls in a row (the shared array keeps the previous call's
+workspace, on calls in a row (the shared array keeps the previous call's
 contents, which must not leak into the next result).  This file is collected
 last, so a stop-at-first-failure run has already run every other test.
 """
@@ -47,11 +47,15 @@ def _call(L, fn, desc, d, H, o, extra):
 @pytest.mark.parametrize("mode,moments", [(M.SWEEP_PER_VIEW, M.MOMENTS_REFERENCE),
                                           (M.SWEEP_AGGREGATED, M.MOMENTS_COMPENSATED)])
 def test_noalloc_matches_workspace_entry_point_twice(cuda, mode, moments):
+    """Three calls in a row on frames of one size with different content: 24
+    planes (one plane chunk: every scratch word written directly), 300 planes
+    (many chunks merged in the scratch, which the call clears first), then 24
+    planes again.  Each must equal mvs_sweep with a fresh caller workspace bit
+    for bit, so nothing of the previous call's scratch reaches a result."""
     import torch
     L = M.lib()
-    results = []
-    # two calls in a row with different frames: the second must not see the first's scratch
-    for seed, (w, h, v, p) in [(31, (96, 72, 3, 40)), (32, (64, 48, 2, 300))]:
+    w, h, v = 96, 72, 3
+    for seed, p in [(31, 24), (32, 300), (33, 24)]:
         fr, planes, d, rel = _inputs(cuda, seed, w, h, v, p, 7)
         desc = M.sweep_desc(w, h, v, len(planes), 7, moments, mode, 1e-4, 0.5, 5.0)
         H = torch.empty(v * len(planes) * 9, device=cuda)
@@ -64,12 +68,12 @@ def test_noalloc_matches_workspace_entry_point_twice(cuda, mode, moments):
         got = _outputs(cuda, desc, n_lab)
         rc = _call(L, "mvs_sweep_noalloc", desc, d, H, got, [None])
         assert rc == 0, L.mvs_last_error()
+        assert L.mvs_last_error() == b""
         torch.cuda.synchronize()
         for k in ("depth", "labels", "best", "cost"):
             if want[k] is not None:
                 np.testing.assert_array_equal(got[k].cpu().numpy(), want[k].cpu().numpy())
-        results.append(got["labels"].cpu().numpy())
-    assert results[0].shape != results[1].shape or not np.array_equal(results[0], results[1])
+        assert (got["labels"].cpu().numpy() >= 0).mean() > 0.5
 
 
 def test_noalloc_rejects_sweeps_beyond_the_fixed_scratch(cuda):
