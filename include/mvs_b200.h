@@ -154,12 +154,25 @@ typedef struct mvs_tgv2_params {
     int32_t niters;       /* iterations per linearisation (reference: niters) */
     int32_t warps;        /* linearisations (reference: warps) */
     double lambda, alpha0, alpha1, tau, sigma, beta, gamma; /* as PlaneSweep::TGV */
-    double tol;           /* extension: stop once |dE| <= tol*|E| between two
-                             checks inside one linearisation; 0 = fixed count */
+    double tol;           /* extension: energy tolerance, 0 = fixed count.  The
+                             energy E (FP64, on the device) is evaluated every
+                             check_every iterations of a linearisation; the run
+                             stops at the first check j >= stop_window with
+                             |E_j - E_{j-W}| <= tol * W * |E_{j-W}|, W =
+                             stop_window: the mean relative change per check
+                             over the last W checks is at most tol.  (The
+                             primal-dual energy is not monotone: a single
+                             check's change dips below tol on the way down.) */
     int32_t check_every;  /* iterations between energy evaluations (tol > 0) */
     int32_t max_iters;    /* extension: total cap (0 = warps * niters) */
     int32_t iteration_kernel; /* MVS_TGV2_ITER_*: how the iterations run (same results) */
+    int32_t stop_window;  /* checks W of the stopping test, 1..MVS_TGV2_STOP_WINDOW_MAX;
+                             0 = MVS_TGV2_STOP_WINDOW_DEFAULT.  W = 1 compares
+                             consecutive checks only. */
 } mvs_tgv2_params;
+
+#define MVS_TGV2_STOP_WINDOW_DEFAULT 5
+#define MVS_TGV2_STOP_WINDOW_MAX 16
 
 #define MVS_TGV2_ITER_AUTO 0     /* the fastest measured form: as MVS_TGV2_ITER_LAUNCH */
 #define MVS_TGV2_ITER_LAUNCH 1   /* one fused launch per iteration (dependent launches, state in

@@ -7,6 +7,15 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Loops whose iterations touch disjoint outputs run over OpenMP threads; the
+ * arithmetic of each element is unchanged, so results do not depend on the
+ * thread count. */
+#ifdef _OPENMP
+#define ORC_PAR _Pragma("omp parallel for schedule(static)")
+#else
+#define ORC_PAR
+#endif
+
 /* Bin centres (fusion.h:1041-1054): -1, linspace over bins 1..N-2, +1. */
 void orc_bin_centers(int bins, float *out)
 {

@@ -35,6 +35,9 @@ extern "C" {
                             R *best, R *depth, int32_t *label);                                 \
     void orc_sweep_ncc_##S(int w, int h, const float *ref, const float *src, const R *H9,       \
                            int winsize, double stdthresh, R *ncc);                              \
+    void orc_sweep_ncc_band_##S(int w, int h, int nview, const float *ref, const float *srcs,       \
+                                const R *H, int nplanes, int winsize, double stdthresh, int y0,  \
+                                int y1, R *out);                                                 \
     void orc_sweep_combine_##S(int w, int h, int nview, const R *best, const R *depth,          \
                                double nccthresh, double zfar, R *out);                          \
     void orc_tensor_##S(int w, int h, const R *img, double beta, double gamma, R *T11, R *T12,  \

@@ -100,6 +100,7 @@ static int FN(mirror)(int k, int n)
 static void FN(box_mean)(int w, int h, const R *in, int win, int squared, R *tmp, R *out)
 {
     const int n = win / 2;
+    ORC_PAR
     for (int y = 0; y < h; ++y)
         for (int x = 0; x < w; ++x) {
             R m = 0;
@@ -109,6 +110,7 @@ static void FN(box_mean)(int w, int h, const R *in, int win, int squared, R *tmp
             }
             tmp[y * w + x] = m / (R)win;
         }
+    ORC_PAR
     for (int y = 0; y < h; ++y)
         for (int x = 0; x < w; ++x) {
             R m = 0;
@@ -129,6 +131,7 @@ static void FN(std_from)(int n, const R *mean, const R *msq, R *std)
 /* transform_indexes_kernel + bilinear_interpolation_kernel_GPU (kernels.cu:4-44) */
 static void FN(warp)(int w, int h, const R *src, const R *H, R *out)
 {
+    ORC_PAR
     for (int k = 0; k < h; ++k)
         for (int l = 0; l < w; ++l) {
             R p[3] = {(R)(l + 1), (R)(k + 1), (R)1}, q[3];
@@ -185,6 +188,7 @@ static void FN(plane_ncc)(int w, int h, const R *srcR, const R *H, int win, R st
     FN(std_from)((int)n, s->wmean, s->wsq, s->wstd);
     for (size_t i = 0; i < n; ++i) s->prod[i] = s->refv[i] * s->warped[i];
     FN(box_mean)(w, h, s->prod, win, 0, s->tmp, s->pmean);
+    ORC_PAR
     for (size_t i = 0; i < n; ++i) {
         if (s->refstd[i] < st || s->wstd[i] < st) ncc[i] = 0;
         else ncc[i] = (s->pmean[i] - s->refmean[i] * s->wmean[i]) / (s->refstd[i] * s->wstd[i]);
@@ -224,6 +228,7 @@ void FN(orc_sweep_view)(int w, int h, const float *ref, const float *src, const 
     FN(ref_moments)(w, h, ref, winsize, &s);
     for (int p = 0; p < nplanes; ++p) {
         FN(plane_ncc)(w, h, srcR, H + 9 * p, winsize, (R)stdthresh, &s, ncc);
+        ORC_PAR
         for (size_t i = 0; i < n; ++i)
             if (ncc[i] > best[i]) {
                 best[i] = ncc[i];
@@ -254,12 +259,101 @@ void FN(orc_sweep_combine)(int w, int h, int nview, const R *best, const R *dept
     }
 }
 
+/* ---- aggregated matching cost over a band of rows ----
+ * For output rows [y0, y1) of a w x h frame: the sum over the nview source
+ * views of the NCC of every plane, computed exactly as orc_sweep_ncc (the
+ * warp, the mirrored box means and calcNCC of kernels.cu:4-64,103-120,187-235)
+ * but only on the rows the band needs: the warped source on rows
+ * [max(0, y0 - r), min(h, y1 + r)), r = winsize / 2, which holds every row the
+ * mirrored column windows of the band read.  Pixels are independent, so the
+ * band equals the same rows of the full-frame computation.  Planes run in
+ * parallel.  H is [nview][nplanes][9]; out is [nplanes][y1 - y0][w]. */
+static void FN(box_mean_band)(int w, int h, const R *in, int lo, int win, int y0, int y1, R *tmp, R *out)
+{
+    const int n = win / 2;
+    for (int y = y0; y < y1; ++y)
+        for (int x = 0; x < w; ++x) {
+            R m = 0;
+            for (int i = -n; i <= n; ++i) m += in[(size_t)(FN(mirror)(y + i, h) - lo) * w + x];
+            tmp[(size_t)(y - y0) * w + x] = m / (R)win;
+        }
+    for (int y = y0; y < y1; ++y)
+        for (int x = 0; x < w; ++x) {
+            R m = 0;
+            for (int i = -n; i <= n; ++i) m += tmp[(size_t)(y - y0) * w + FN(mirror)(x + i, w)];
+            out[(size_t)(y - y0) * w + x] = m / (R)win;
+        }
+}
+
+static void FN(warp_rows)(int w, int h, const float *src, const R *H, int lo, int hi, R *out)
+{
+    for (int k = lo; k < hi; ++k)
+        for (int l = 0; l < w; ++l) {
+            R p[3] = {(R)(l + 1), (R)(k + 1), (R)1}, q[3];
+            FN(matvec)(H, p, q);
+            R xs = q[0] / q[2] - 1, ys = q[1] / q[2] - 1;
+            R fx = FLOORR(xs), fy = FLOORR(ys);
+            R v = 0;
+            if (fx >= 0 && fy >= 0 && fx + 1 <= (R)(w - 1) && fy + 1 <= (R)(h - 1)) {
+                int ix = (int)fx, iy = (int)fy;
+                R a = xs - (R)ix, b = ys - (R)iy;
+                R t1 = a * (R)src[iy * w + ix + 1] + (1 - a) * (R)src[iy * w + ix];
+                R t2 = a * (R)src[(iy + 1) * w + ix + 1] + (1 - a) * (R)src[(iy + 1) * w + ix];
+                v = b * t2 + (1 - b) * t1;
+            }
+            out[(size_t)(k - lo) * w + l] = v;
+        }
+}
+
+void FN(orc_sweep_ncc_band)(int w, int h, int nview, const float *ref, const float *srcs, const R *H, int nplanes,
+                            int winsize, double stdthresh, int y0, int y1, R *out)
+{
+    const int r = winsize / 2, lo = y0 - r > 0 ? y0 - r : 0, hi = y1 + r < h ? y1 + r : h;
+    const size_t nb = (size_t)(y1 - y0) * w, nr = (size_t)(hi - lo) * w;
+    const R st = (R)stdthresh;
+    R *refv = (R *)malloc(nr * sizeof(R)), *rm = (R *)malloc(nb * sizeof(R)), *rs = (R *)malloc(nb * sizeof(R)),
+      *t0 = (R *)malloc(nb * sizeof(R)), *sq = (R *)malloc(nr * sizeof(R));
+    for (size_t i = 0; i < nr; ++i) {
+        refv[i] = (R)ref[(size_t)lo * w + i];
+        sq[i] = refv[i] * refv[i];
+    }
+    FN(box_mean_band)(w, h, refv, lo, winsize, y0, y1, t0, rm);
+    FN(box_mean_band)(w, h, sq, lo, winsize, y0, y1, t0, rs);
+    FN(std_from)((int)nb, rm, rs, rs);
+    free(t0);
+    free(sq);
+#pragma omp parallel for schedule(dynamic)
+    for (int p = 0; p < nplanes; ++p) {
+        R *wp = (R *)malloc(nr * sizeof(R)), *w2 = (R *)malloc(nr * sizeof(R)), *pr = (R *)malloc(nr * sizeof(R)),
+          *tmp = (R *)malloc(nb * sizeof(R)), *wm = (R *)malloc(nb * sizeof(R)), *wq = (R *)malloc(nb * sizeof(R)),
+          *pm = (R *)malloc(nb * sizeof(R));
+        R *o = out + (size_t)p * nb;
+        for (size_t i = 0; i < nb; ++i) o[i] = 0;
+        for (int v = 0; v < nview; ++v) {
+            FN(warp_rows)(w, h, srcs + (size_t)v * w * h, H + ((size_t)v * nplanes + p) * 9, lo, hi, wp);
+            for (size_t i = 0; i < nr; ++i) {
+                w2[i] = wp[i] * wp[i];
+                pr[i] = refv[i] * wp[i];
+            }
+            FN(box_mean_band)(w, h, wp, lo, winsize, y0, y1, tmp, wm);
+            FN(box_mean_band)(w, h, w2, lo, winsize, y0, y1, tmp, wq);
+            FN(box_mean_band)(w, h, pr, lo, winsize, y0, y1, tmp, pm);
+            FN(std_from)((int)nb, wm, wq, wq);
+            for (size_t i = 0; i < nb; ++i)
+                if (!(rs[i] < st || wq[i] < st)) o[i] += (pm[i] - rm[i] * wm[i]) / (rs[i] * wq[i]);
+        }
+        free(wp); free(w2); free(pr); free(tmp); free(wm); free(wq); free(pm);
+    }
+    free(refv); free(rm); free(rs);
+}
+
 /* ---- TGV2: TGV2_kernels.cu, planesweep.cpp:381-536 ---- */
 
 /* Anisotropic_diffusion_tensor_kernel, TGV2_kernels.cu:257-298 */
 void FN(orc_tensor)(int w, int h, const R *img, double beta, double gamma, R *T11, R *T12, R *T21, R *T22)
 {
     const R bt = (R)beta, gm = (R)gamma;
+    ORC_PAR
     for (int y = 0; y < h; ++y)
         for (int x = 0; x < w; ++x) {
             int i = y * w + x, xn = x + 1 < w - 1 ? x + 1 : w - 1, yn = y + 1 < h - 1 ? y + 1 : h - 1;
@@ -298,6 +392,7 @@ void FN(orc_tgv2_linearize)(int w, int h, const R *src01, const R *ref01, const 
     const R fx = K[0], fy = K[4];
     R RinvK[9];
     FN(matmul)(Rrel, invK, RinvK);
+    ORC_PAR
     for (int k = 0; k < h; ++k)
         for (int l = 0; l < w; ++l) {
             const int i = k * w + l;
@@ -317,6 +412,7 @@ void FN(orc_tgv2_linearize)(int w, int h, const R *src01, const R *ref01, const 
             dfy[i] = fy * (dX[1] * Z[i] - Y[i] * dX[2]) / (Z[i] * Z[i]);
         }
     /* bilinear_interpolation at the transformed coordinates (kernels.cu:4-29) */
+    ORC_PAR
     for (int k = 0; k < h; ++k)
         for (int l = 0; l < w; ++l) {
             const int i = k * w + l;
@@ -331,6 +427,7 @@ void FN(orc_tgv2_linearize)(int w, int h, const R *src01, const R *ref01, const 
             R t2 = aa * src01[(iy + 1) * w + ix + 1] + (1 - aa) * src01[(iy + 1) * w + ix];
             Iw[i] = bb * t2 + (1 - bb) * t1;
         }
+    ORC_PAR
     for (int y = 0; y < h; ++y)
         for (int x = 0; x < w; ++x) {
             int i = y * w + x, xn = x + 1 < w - 1 ? x + 1 : w - 1, yn = y + 1 < h - 1 ? y + 1 : h - 1;
@@ -354,6 +451,7 @@ void FN(orc_tgv2_iteration)(int w, int h, int nview, const R *T11, const R *T12,
 {
     const size_t n = (size_t)w * h;
     const R lambda = (R)lambda_, alpha0 = (R)alpha0_, alpha1 = (R)alpha1_, tau = (R)tau_, sigma = (R)sigma_;
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
@@ -365,6 +463,7 @@ void FN(orc_tgv2_iteration)(int w, int h, int nview, const R *T11, const R *T12,
             Px[i] = (R)(dx / d);
             Py[i] = (R)(dy / d);
         }
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
@@ -386,12 +485,14 @@ void FN(orc_tgv2_iteration)(int w, int h, int nview, const R *T11, const R *T12,
     for (int v = 0; v < nview; ++v) {
         R *rv = r + (size_t)v * n;
         const R *itv = It + (size_t)v * n, *iuv = Iu + (size_t)v * n;
+        ORC_PAR
         for (size_t i = 0; i < n; ++i) {
             rv[i] = rv[i] + sigma * lambda * (itv[i] + (u[i] - u0[i]) * iuv[i]);
             rv[i] = rv[i] / FMAXR(1, FABSR(rv[i]));
             prodsum[i] += rv[i] * iuv[i];
         }
     }
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xp = xx - 1 > 0 ? xx - 1 : 0, yp = yy - 1 > 0 ? yy - 1 : 0;
@@ -423,8 +524,12 @@ double FN(orc_tgv2_energy)(int w, int h, int nview, const R *T11, const R *T12, 
                            double lambda, double alpha0, double alpha1)
 {
     const size_t n = (size_t)w * h;
-    double e1 = 0, e0 = 0, ed = 0;
-    for (int yy = 0; yy < h; ++yy)
+    /* per-row partial sums, added in row order: the same result for any
+     * number of threads */
+    double *rows = (double *)calloc((size_t)3 * h, sizeof(double));
+    ORC_PAR
+    for (int yy = 0; yy < h; ++yy) {
+        double e1 = 0, e0 = 0, ed = 0;
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
             double gx = (double)u[yy * w + xn] - u[i] - u1x[i];
@@ -437,6 +542,17 @@ double FN(orc_tgv2_energy)(int w, int h, int nview, const R *T11, const R *T12, 
             for (int v = 0; v < nview; ++v)
                 ed += fabs((double)It[v * n + i] + ((double)u[i] - u0[i]) * Iu[v * n + i]);
         }
+        rows[3 * yy] = e1;
+        rows[3 * yy + 1] = e0;
+        rows[3 * yy + 2] = ed;
+    }
+    double e1 = 0, e0 = 0, ed = 0;
+    for (int yy = 0; yy < h; ++yy) {
+        e1 += rows[3 * yy];
+        e0 += rows[3 * yy + 1];
+        ed += rows[3 * yy + 2];
+    }
+    free(rows);
     return alpha1 * e1 + alpha0 * e0 + lambda * ed;
 }
 
@@ -453,6 +569,7 @@ void FN(orc_tgv_sparse_iteration)(int w, int h, const R *T11, const R *T12, cons
                                   R *Qz, R *Qw, double alpha0_, double alpha1_, double tau_, double sigma_)
 {
     const R alpha0 = (R)alpha0_, alpha1 = (R)alpha1_, tau = (R)tau_, sigma = (R)sigma_;
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
@@ -464,6 +581,7 @@ void FN(orc_tgv_sparse_iteration)(int w, int h, const R *T11, const R *T12, cons
             Px[i] = (R)(dx / d);
             Py[i] = (R)(dy / d);
         }
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
@@ -481,6 +599,7 @@ void FN(orc_tgv_sparse_iteration)(int w, int h, const R *T11, const R *T12, cons
             Qz[i] = (R)(dz / d);
             Qw[i] = (R)(dw / d);
         }
+    ORC_PAR
     for (int yy = 0; yy < h; ++yy)
         for (int xx = 0; xx < w; ++xx) {
             int i = yy * w + xx, xp = xx - 1 > 0 ? xx - 1 : 0, yp = yy - 1 > 0 ? yy - 1 : 0;
@@ -521,6 +640,7 @@ void FN(orc_tvl1_denoise)(int w, int h, const R *ref255, const R *depth, double 
     for (int it = 0; it < niters; ++it) {
         const R cs = (R)(it == 0 ? 1 + sigma_ : sigma_);
         /* denoising_TVL1_calculateP_tensor_weighed_kernel, kernels.cu:283-307 */
+        ORC_PAR
         for (int yy = 0; yy < h; ++yy)
             for (int xx = 0; xx < w; ++xx) {
                 int i = yy * w + xx, xn = xx + 1 < w - 1 ? xx + 1 : w - 1, yn = yy + 1 < h - 1 ? yy + 1 : h - 1;
@@ -533,6 +653,7 @@ void FN(orc_tvl1_denoise)(int w, int h, const R *ref255, const R *depth, double 
                 Py[i] = (R)(dy / d);
             }
         /* denoising_TVL1_update_kernel, kernels.cu:342-370 */
+        ORC_PAR
         for (int yy = 0; yy < h; ++yy)
             for (int xx = 0; xx < w; ++xx) {
                 int i = yy * w + xx, yp = yy - 1 < 0 ? 0 : yy - 1;
@@ -563,6 +684,7 @@ void FN(orc_fusion_histogram)(int bins, int vw, int vh, int vd, const float *a, 
     const R ax = (R)a[0], ay = (R)a[1], az = (R)a[2];
     const R sx = (R)b[0] - ax, sy = (R)b[1] - ay, sz = (R)b[2] - az;
     const R thr = bins == 2 ? 0 : (R)thr_;
+    ORC_PAR
     for (int z = 0; z < vd; ++z)
         for (int y = 0; y < vh; ++y)
             for (int x = 0; x < vw; ++x) {
@@ -605,6 +727,7 @@ void FN(orc_fusion_u)(int bins, int vw, int vh, int vd, const uint16_t *hist, R 
     const R *px = p, *py = p + n, *pz = p + 2 * n;
     float centers[16];
     orc_bin_centers(bins, centers);
+    ORC_PAR
     for (int z = 0; z < vd; ++z)
         for (int y = 0; y < vh; ++y)
             for (int x = 0; x < vw; ++x) {
@@ -623,24 +746,40 @@ void FN(orc_fusion_u)(int bins, int vw, int vh, int vd, const uint16_t *hist, R 
 #else
                 {
                     /* the same selection in double: values below the smallest
-                     * element are raised to it, as the float insertion does */
-                    double vals[33];
-                    int m = 0;
-                    for (int k = 0; k < bins; ++k) vals[m++] = centers[k];
-                    double lo = centers[0];
-                    vals[m++] = uu < lo ? lo : uu;
+                     * element are raised to it, as the float insertion does.
+                     * The median (rank N of the 2N+1 values) is taken by a
+                     * merge of the sorted bin centres, the sorted proximal
+                     * points u + tau lambda W_j and u itself. */
+                    const double lo = centers[0];
+                    double pts[16];
+                    long W = 0;
+                    for (int k = 1; k <= bins; ++k) W += hh[k - 1];
                     for (int j = 1; j <= bins; ++j) {
-                        long W = 0;
-                        for (int k = 1; k <= j; ++k) W -= hh[k - 1];
-                        for (int k = j + 1; k <= bins; ++k) W += hh[k - 1];
+                        W -= 2 * (long)hh[j - 1];   /* W_j = -sum_{k<=j} h_k + sum_{k>j} h_k */
                         double pj = uu + tau * lambda * (double)W;
-                        vals[m++] = pj < lo ? lo : pj;
-                    }
-                    for (int a1 = 1; a1 < m; ++a1)
-                        for (int b1 = a1; b1 > 0 && vals[b1] < vals[b1 - 1]; --b1) {
-                            double tt = vals[b1]; vals[b1] = vals[b1 - 1]; vals[b1 - 1] = tt;
+                        pj = pj < lo ? lo : pj;
+                        int b1 = j - 1;
+                        while (b1 > 0 && pts[b1 - 1] > pj) {
+                            pts[b1] = pts[b1 - 1];
+                            --b1;
                         }
-                    unew = vals[bins];
+                        pts[b1] = pj;
+                    }
+                    const double uc = uu < lo ? lo : uu;
+                    int ia = 0, ib = 0, took_u = 0;
+                    double cur = 0;
+                    for (int k = 0; k <= bins; ++k) {
+                        const double ca = ia < bins ? (double)centers[ia] : INFINITY;
+                        const double cb = ib < bins ? pts[ib] : INFINITY;
+                        const double cu = took_u ? INFINITY : uc;
+                        if (ca <= cb && ca <= cu) cur = centers[ia++];
+                        else if (cb <= cu) cur = pts[ib++];
+                        else {
+                            cur = cu;
+                            took_u = 1;
+                        }
+                    }
+                    unew = cur;
                 }
 #endif
                 u[i] = unew;
@@ -655,6 +794,7 @@ void FN(orc_fusion_p)(int vw, int vh, int vd, const R *v, R *p, double sigma_)
     const size_t n = (size_t)vw * vh * vd, sy = vw, sz = (size_t)vw * vh;
     R *px = p, *py = p + n, *pz = p + 2 * n;
     const R sigma = (R)sigma_;
+    ORC_PAR
     for (int z = 0; z < vd; ++z)
         for (int y = 0; y < vh; ++y)
             for (int x = 0; x < vw; ++x) {
@@ -675,6 +815,7 @@ void FN(orc_fusion_p)(int vw, int vh, int vd, const R *v, R *p, double sigma_)
  * for z < 5.5, else z = -9. */
 void FN(orc_compute3d)(int w, int h, const R *depth, const R *invK, const R *Rr, const R *t, R *X, R *Y, R *Z)
 {
+    ORC_PAR
     for (int y = 0; y < h; ++y)
         for (int x = 0; x < w; ++x) {
             int i = y * w + x;

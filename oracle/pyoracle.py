@@ -77,6 +77,8 @@ def _declare_oracle(L):
         getattr(L, f"orc_sweep_view_{S}").argtypes = [C.c_int, C.c_int, _F, _F, P, _F, C.c_int, C.c_int,
                                                       C.c_double, P, P, _I]
         getattr(L, f"orc_sweep_ncc_{S}").argtypes = [C.c_int, C.c_int, _F, _F, P, C.c_int, C.c_double, P]
+        getattr(L, f"orc_sweep_ncc_band_{S}").argtypes = [C.c_int, C.c_int, C.c_int, _F, _F, P, C.c_int, C.c_int,
+                                                          C.c_double, C.c_int, C.c_int, P]
         getattr(L, f"orc_sweep_combine_{S}").argtypes = [C.c_int, C.c_int, C.c_int, P, P, C.c_double,
                                                          C.c_double, P]
         getattr(L, f"orc_tensor_{S}").argtypes = [C.c_int, C.c_int, P, C.c_double, C.c_double, P, P, P, P]
@@ -192,6 +194,22 @@ def sweep(ref, srcs, H, depths, winsize, stdthresh=1e-4, nccthresh=0.5, zfar=1.0
     out = np.zeros((h, w), dt)
     getattr(L, f"orc_sweep_combine_{precision}")(w, h, V, P(best), P(vdepth), nccthresh, zfar, P(out))
     return dict(depth=out, best=best, vdepth=vdepth, label=label)
+
+
+def sweep_ncc_band(ref, srcs, H, winsize, y0, y1, stdthresh=1e-4, precision="f64"):
+    """Sum over the source views of every plane's NCC on output rows [y0, y1):
+    (nplanes, y1 - y0, W), as orc_sweep_ncc computes each view on the full
+    frame.  H is (nviews, nplanes, 9)."""
+    L = oracle_lib()
+    dt = np.float32 if precision == "f32" else np.float64
+    P = _fp if precision == "f32" else _dp
+    h, w = ref.shape
+    V, NP = H.shape[0], H.shape[1]
+    out = np.zeros((NP, y1 - y0, w), dt)
+    getattr(L, f"orc_sweep_ncc_band_{precision}")(w, h, V, _fp(_f32(ref)), _fp(_f32(np.stack(srcs))),
+                                                  P(np.ascontiguousarray(H, dt)), NP, winsize, stdthresh, y0, y1,
+                                                  P(out))
+    return out
 
 
 def ref_sweep(ref, srcs, K_1based, Rref, tref, src_poses, planes, winsize, znear=0.1, zfar=1.0,
@@ -382,11 +400,13 @@ def tgv2_linearize(setup, u0, precision="f64"):
 
 def tgv2(ref255, srcs255, K_1based, Rref, tref, src_poses, niters=30, warps=15, lam=0.5, alpha0=2.0,
          alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0, u_init=None, alternative=False,
-         precision="f64", tol=0.0, check_every=10, max_iters=None):
+         precision="f64", tol=0.0, check_every=10, max_iters=None, stop_window=5):
     """PlaneSweep::TGV (planesweep.cpp:381-536) driven from Python over the C
-    kernels.  With ``tol > 0`` the run also stops once the relative change of
-    the energy between two checks ``check_every`` iterations apart (inside one
-    linearisation) falls below ``tol``; ``max_iters`` caps the total count.
+    kernels.  With ``tol > 0`` the energy E_j is evaluated every
+    ``check_every`` iterations of a linearisation and the run stops at the
+    first check j >= W with |E_j - E_{j-W}| <= tol * W * |E_{j-W}|, W =
+    ``stop_window`` (the stopping rule of mvs_tgv2_params); ``max_iters``
+    caps the total count.
 
     Returns (u, iterations, energies)."""
     L = oracle_lib()
@@ -410,7 +430,7 @@ def tgv2(ref255, srcs255, K_1based, Rref, tref, src_poses, niters=30, warps=15, 
             getattr(S, f)[:] = 0
         S.r[:] = 0
         It, Iu = tgv2_linearize(st, S.u0, precision)
-        prev = None
+        hist = []
         for k in range(niters):
             it_fn(w, h, V, *[P(t) for t in T], P(It), P(Iu), P(S.u0), P(S.u), P(S.u1x), P(S.u1y), P(S.ubar),
                   P(S.u1xbar), P(S.u1ybar), P(S.Px), P(S.Py), P(S.Qx), P(S.Qy), P(S.Qz), P(S.Qw), P(S.r),
@@ -420,12 +440,78 @@ def tgv2(ref255, srcs255, K_1based, Rref, tref, src_poses, niters=30, warps=15, 
                 E = en_fn(w, h, V, *[P(t) for t in T], P(It), P(Iu), P(S.u0), P(S.u), P(S.u1x), P(S.u1y),
                           lam, alpha0, alpha1)
                 energies.append(E)
-                if prev is not None and abs(prev - E) <= tol * abs(prev):
+                hist.append(E)
+                if len(hist) > stop_window and abs(hist[-1 - stop_window] - E) <= tol * stop_window * abs(
+                        hist[-1 - stop_window]):
                     done = True
                     break
-                prev = E
             if total >= cap:
                 done = True
+                break
+    return S.u.copy(), total, energies
+
+
+def tgv2_warm(ref255, srcs255, K_1based, Rref, tref, src_poses, u_lin, u_start, v_start, dual_sigma, dual_sigma_r,
+              max_iters=500, lam=0.5, alpha0=2.0, alpha1=1.5, tau=0.008, sigma=2.5, beta=0.0, gamma=1.0,
+              tol=1e-4, check_every=10, stop_window=5, alternative=False):
+    """A warm-started TGV2 run as mvs_tgv2_run_warm makes it, in FP64 (one
+    linearisation): the data term linearised at ``u_lin``, the primal started
+    at ``u_start`` and ``v_start`` (2, H, W), the duals one dual step of size
+    ``dual_sigma`` (p, q) and ``dual_sigma_r`` (r) from zero with the
+    iteration's own operators and projections (P of TGV2_kernels.cu:340-365,
+    Q of :54-85, R of :87-105), then the iterations of PlaneSweep::TGV with the
+    given steps and the same stopping rule as ``tgv2``.
+
+    Returns (u, iterations, energies)."""
+    L = oracle_lib()
+    precision = "f64"
+    st = tgv2_setup(ref255, srcs255, K_1based, Rref, tref, src_poses, alternative, precision)
+    P, dt = st["P"], st["dt"]
+    h, w = st["ref01"].shape
+    V = len(srcs255)
+    T = tensor(st["ref01"], beta, gamma, precision)
+    S = TGV2State(h, w, V, dt)
+    S.u0[:] = u_lin
+    S.u[:] = u_start
+    S.ubar[:] = S.u
+    S.u1x[:] = v_start[0]
+    S.u1y[:] = v_start[1]
+    S.u1xbar[:] = S.u1x
+    S.u1ybar[:] = S.u1y
+    It, Iu = tgv2_linearize(st, S.u0, precision)
+    xn = np.minimum(np.arange(w) + 1, w - 1)
+    yn = np.minimum(np.arange(h) + 1, h - 1)
+    u, vx, vy = (np.asarray(a, np.float64) for a in (S.u, S.u1x, S.u1y))
+    T11, T12, T21, T22 = (np.asarray(t, np.float64) for t in T)
+    if dual_sigma > 0:
+        xg, yg = u[:, xn] - u - vx, u[yn, :] - u - vy
+        sc = alpha1 * dual_sigma
+        dx, dy = sc * (T11 * xg + T12 * yg), sc * (T21 * xg + T22 * yg)
+        d = np.maximum(1.0, np.sqrt(dx * dx + dy * dy))
+        S.Px[:], S.Py[:] = dx / d, dy / d
+        sc = alpha0 * dual_sigma
+        dx, dy = sc * (vx[:, xn] - vx), sc * (vy[yn, :] - vy)
+        dz = sc * ((vx[yn, :] - vx) + (vy[:, xn] - vy)) / 2.0
+        d = np.maximum(1.0, np.sqrt(dx * dx + dy * dy + 2 * dz * dz))
+        S.Qx[:], S.Qy[:], S.Qz[:], S.Qw[:] = dx / d, dy / d, dz / d, dz / d
+    if dual_sigma_r > 0:
+        q = dual_sigma_r * lam * (np.asarray(It, np.float64) + (u - np.asarray(S.u0, np.float64)) * Iu)
+        S.r[:] = q / np.maximum(1.0, np.abs(q))
+    it_fn = getattr(L, f"orc_tgv2_iteration_{precision}")
+    en_fn = getattr(L, f"orc_tgv2_energy_{precision}")
+    total, energies, hist = 0, [], []
+    for k in range(max_iters):
+        it_fn(w, h, V, *[P(t) for t in T], P(It), P(Iu), P(S.u0), P(S.u), P(S.u1x), P(S.u1y), P(S.ubar),
+              P(S.u1xbar), P(S.u1ybar), P(S.Px), P(S.Py), P(S.Qx), P(S.Qy), P(S.Qz), P(S.Qw), P(S.r),
+              P(S.prodsum), lam, alpha0, alpha1, tau, sigma)
+        total += 1
+        if tol > 0 and (k + 1) % check_every == 0:
+            E = en_fn(w, h, V, *[P(t) for t in T], P(It), P(Iu), P(S.u0), P(S.u), P(S.u1x), P(S.u1y), lam,
+                      alpha0, alpha1)
+            energies.append(E)
+            hist.append(E)
+            if len(hist) > stop_window and abs(hist[-1 - stop_window] - E) <= tol * stop_window * abs(
+                    hist[-1 - stop_window]):
                 break
     return S.u.copy(), total, energies
 

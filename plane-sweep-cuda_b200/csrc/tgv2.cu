@@ -193,13 +193,29 @@ __global__ void linearize_kernel(Cams c, const float *__restrict__ srcs255, cons
 // at that check.
 struct IterCtl {
     int done;          // the tolerance was met
-    int have_prev;     // an energy of this linearisation was evaluated
+    int n_hist;        // energies evaluated in this linearisation
     int have_energy;   // last_e holds an energy
     int stop_total;    // iteration count at which the tolerance was met
     int energy_at;     // iteration count at which last_e was evaluated
     unsigned int blocks_done;   // energy_kernel blocks finished (the last one resets it)
-    double prev, last_e;
+    double last_e;
+    double hist[MVS_TGV2_STOP_WINDOW_MAX];   // the last energies, hist[j % MAX] = E_j
 };
+
+// The stopping test at check j of a linearisation (E_j = E, `hist` holding
+// E_{j-W} .. E_{j-1} in ring order, `n` = j): the mean relative change per
+// check over the last W checks is at most tol.  Records E_j.  W <= MAX, so
+// E_{j-W} is read before E_j replaces it in the ring.
+__device__ __forceinline__ bool stop_test(double *hist, int n, double E, double tol, int W)
+{
+    bool met = false;
+    if (n >= W) {
+        const double old = hist[(n - W) % MVS_TGV2_STOP_WINDOW_MAX];
+        met = fabs(old - E) <= tol * (double)W * fabs(old);
+    }
+    hist[n % MVS_TGV2_STOP_WINDOW_MAX] = E;
+    return met;
+}
 
 struct IterBufs {
     const IterCtl *ctl;   // null: no stopping test
@@ -389,15 +405,16 @@ constexpr int EB = 256;
 // P, Q and R updates.  Each block adds its pixels' terms; the block that
 // finishes last (a completion counter, nothing waits) adds the blocks' partial
 // sums in block order, writes the energy and, given `ctl`, applies the
-// stopping test of the launch path: |E_prev - E| <= tol |E_prev| between two
-// checks of one linearisation.  Launches after a met tolerance return at once.
+// stopping test of the launch path (stop_test over the checks of one
+// linearisation).  Launches after a met tolerance return at once.
 __global__ void __launch_bounds__(EB) energy_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
                                                     const float *__restrict__ T22, const float *__restrict__ It,
                                                     const float *__restrict__ Iu, const float *__restrict__ u0,
                                                     const float *__restrict__ u, const float *__restrict__ u1x,
                                                     const float *__restrict__ u1y, int w, int h, int V, double lambda,
                                                     double alpha0, double alpha1, double *__restrict__ partial,
-                                                    double *__restrict__ out, IterCtl *ctl, double tol, int total)
+                                                    double *__restrict__ out, IterCtl *ctl, double tol, int total,
+                                                    int window)
 {
     __shared__ double red[EB / 32];
     __shared__ int last;
@@ -446,13 +463,11 @@ __global__ void __launch_bounds__(EB) energy_kernel(const float *__restrict__ T1
         for (int k = 0; k < EB / 32; ++k) E += red[k];
         *out = E;
         if (tol > 0) {
-            if (ctl->have_prev && fabs(ctl->prev - E) <= tol * fabs(ctl->prev)) {
+            if (stop_test(ctl->hist, ctl->n_hist, E, tol, window)) {
                 ctl->done = 1;
                 ctl->stop_total = total;
-            } else {
-                ctl->prev = E;
-                ctl->have_prev = 1;
             }
+            ++ctl->n_hist;
             ctl->last_e = E;
             ctl->have_energy = 1;
             ctl->energy_at = total;
@@ -549,7 +564,7 @@ struct PersistBufs {
     double *partial;                           // [grid]
     unsigned int *bar;                         // count, generation, abort
     PersistResult *res;
-    int w, h, V, tiles_x, th, niters, cap_left, check_every;
+    int w, h, V, tiles_x, th, niters, cap_left, check_every, stop_window;
     double tol;
     float lambda, alpha0, alpha1, tau, sigma;
     double dlambda, dalpha0, dalpha1;
@@ -654,8 +669,10 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
 
     const float a1s = b.alpha1 * b.sigma, a0s = b.alpha0 * b.sigma, sl = b.sigma * b.lambda;
     const int limit = min(b.niters, b.cap_left);
-    int k = 0, energy_at = -1, have_prev = 0, done = 0;
-    double last_e = 0.0, prev = 0.0;
+    int k = 0, energy_at = -1, n_hist = 0, done = 0;
+    double last_e = 0.0;
+    __shared__ double s_hist[MVS_TGV2_STOP_WINDOW_MAX];   // energies of this launch's checks (thread 0)
+    __shared__ int s_met;
     bool ok = true;
     while (k < limit) {
         const int par = k & 1;
@@ -874,16 +891,16 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
                 double t = 0.0;
                 for (unsigned int q = 0; q < nblocks; ++q) t += __ldcg(b.partial + q);
                 s_e = t;
+                s_met = stop_test(s_hist, n_hist, t, b.tol, b.stop_window);
             }
             __syncthreads();
             last_e = s_e;
             energy_at = k;
-            if (have_prev && fabs(prev - last_e) <= b.tol * fabs(prev)) {
+            ++n_hist;
+            if (s_met) {
                 done = 1;
                 break;
             }
-            prev = last_e;
-            have_prev = 1;
         }
     }
     if (ok) {
@@ -1226,6 +1243,9 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
              float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st, const TGV2Warm *warm)
 {
     if (V > kMaxViews) return set_error(MVS_ERR_ARG, "at most %d views", kMaxViews);
+    if (prm->stop_window < 0 || prm->stop_window > MVS_TGV2_STOP_WINDOW_MAX)
+        return set_error(MVS_ERR_ARG, "stop_window %d: 0 (default) or 1..%d", prm->stop_window,
+                         MVS_TGV2_STOP_WINDOW_MAX);
     Layout L = layout(ws, w, h, V);
     const int n = w * h;
     Cams cams;
@@ -1246,6 +1266,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
 
     const int cap = prm->max_iters > 0 ? prm->max_iters : prm->warps * prm->niters;
     const int check_every = prm->check_every > 0 ? prm->check_every : 10;
+    const int stop_window = prm->stop_window > 0 ? prm->stop_window : MVS_TGV2_STOP_WINDOW_DEFAULT;
     // the energy is read back into pageable host memory: a synchronous 8-byte
     // copy needs no pinned staging (allocating one per call costs milliseconds)
     double host_energy = 0.0;
@@ -1318,7 +1339,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     MVS_TRY_CUDA(cudaMemsetAsync(L.ctl, 0, sizeof(IterCtl), st));
     for (int l = 0; l < prm->warps && !done; ++l) {
         if (!pth && prm->tol > 0 && l > 0)   // a new linearisation has no previous energy
-            MVS_TRY_CUDA(cudaMemsetAsync(&L.ctl->have_prev, 0, sizeof(int), st));
+            MVS_TRY_CUDA(cudaMemsetAsync(&L.ctl->n_hist, 0, sizeof(int), st));
         if (warm && l == 0)
             warm_init_kernel<<<eg, 256, 0, st>>>(n, V, warm->u_lin, u, warm->v, warm->v ? warm->v + n : nullptr, L.u0,
                                                 L.ubar[0], L.u1x, L.u1y, L.u1xbar[0], L.u1ybar[0], L.Px[0], L.Py[0],
@@ -1375,6 +1396,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             pb.niters = prm->niters;
             pb.cap_left = cap - total;
             pb.check_every = check_every;
+            pb.stop_window = stop_window;
             pb.tol = prm->tol;
             pb.lambda = prm->lambda;
             pb.alpha0 = prm->alpha0;
@@ -1436,7 +1458,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
                 MVS_TRY_CUDA(launch_dependent(energy_kernel, dim3(energy_blocks(n)), dim3(EB), 0, st, L.T11, L.T12,
                                               L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V, prm->lambda,
                                               prm->alpha0, prm->alpha1, L.partial, L.energy, L.ctl, prm->tol,
-                                              launched));
+                                              launched, stop_window));
             }
             if (launched >= cap) {
                 done = true;
@@ -1484,7 +1506,7 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         // energy of the final iterate for callers that ask for it
         energy_kernel<<<energy_blocks(n), EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h,
                                                       V, prm->lambda, prm->alpha0, prm->alpha1, L.partial, L.energy,
-                                                      L.ctl, 0.0, total);
+                                                      L.ctl, 0.0, total, 1);
         cudaMemcpyAsync(h_energy, L.energy, sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = set_error(MVS_ERR_CUDA, "tgv2 energy: %s", cudaGetErrorString(e));

@@ -98,7 +98,7 @@ class TGV2Params(C.Structure):
     _fields_ = [("niters", C.c_int32), ("warps", C.c_int32), ("lam", C.c_double), ("alpha0", C.c_double),
                 ("alpha1", C.c_double), ("tau", C.c_double), ("sigma", C.c_double), ("beta", C.c_double),
                 ("gamma", C.c_double), ("tol", C.c_double), ("check_every", C.c_int32), ("max_iters", C.c_int32),
-                ("iteration_kernel", C.c_int32)]
+                ("iteration_kernel", C.c_int32), ("stop_window", C.c_int32)]
 
 
 class TVL1Params(C.Structure):
@@ -309,10 +309,17 @@ def sweep_wta_volume(cost, depths, n_pixels, n_planes, zfar, depth_out, labels=N
 TGV2_ITER_AUTO, TGV2_ITER_LAUNCH, TGV2_ITER_PERSISTENT = 0, 1, 2
 
 
+TGV2_STOP_WINDOW_DEFAULT = 5
+
+
 def tgv2_params(niters=30, warps=15, lam=0.5, alpha0=2.0, alpha1=1.5, tau=0.02, sigma=1.0, beta=0.0, gamma=1.0,
-                tol=0.0, check_every=10, max_iters=0, iteration_kernel=TGV2_ITER_AUTO):
+                tol=0.0, check_every=10, max_iters=0, iteration_kernel=TGV2_ITER_AUTO,
+                stop_window=TGV2_STOP_WINDOW_DEFAULT):
+    """mvs_tgv2_params.  With tol > 0 the run stops at the first energy check
+    j >= stop_window where |E_j - E_{j-W}| <= tol * W * |E_{j-W}| (W =
+    stop_window; checks every check_every iterations of a linearisation)."""
     return TGV2Params(niters, warps, lam, alpha0, alpha1, tau, sigma, beta, gamma, tol, check_every, max_iters,
-                      iteration_kernel)
+                      iteration_kernel, stop_window)
 
 
 def float_cams(K_1based, rel_poses):

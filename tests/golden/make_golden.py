@@ -57,13 +57,16 @@ def sweep_case(name, seed, w, h, n_src, n_planes, win, planes_kind, znear=0.5, z
                         label=po.labels_from_depth(r["vdepth"], pl))
 
 
-def tgv_case(name, seed, w, h, n_src, niters, warps, start):
+def tgv_case(name, seed, w, h, n_src, niters, warps, start, beta=0.0, gamma=1.0):
+    """PlaneSweep::TGV; beta != 0 turns the anisotropic diffusion tensor on
+    (TGV2_kernels.cu:257-298), which then weights the P and U steps."""
     fr, _, _ = scenes.config_tiny(seed=seed, width=w, height=h, n_src=n_src)
     a = frame_arrays(fr)
     u_init = None if start == "one" else a["depth_gt"]
     u, _ = po.ref_tgv(a["ref"], list(a["srcs"]), a["K"], a["Rref"], a["tref"], poses(a), niters=niters, warps=warps,
-                      u_init=u_init)
-    np.savez_compressed(HERE / f"{name}.npz", **a, niters=niters, warps=warps, start=start, u=u)
+                      u_init=u_init, beta=beta, gamma=gamma)
+    np.savez_compressed(HERE / f"{name}.npz", **a, niters=niters, warps=warps, start=start, beta=beta, gamma=gamma,
+                        u=u)
 
 
 def tvl1_case(name, seed, w, h, niters):
@@ -136,6 +139,7 @@ def main(only=None):
                nccthresh=-0.25)
     tgv_case("tgv_from_one", seed=21, w=48, h=40, n_src=2, niters=10, warps=3, start="one")
     tgv_case("tgv_from_depth", seed=22, w=48, h=40, n_src=3, niters=25, warps=2, start="depth")
+    tgv_case("tgv_aniso", seed=23, w=56, h=44, n_src=3, niters=20, warps=2, start="depth", beta=1.5, gamma=0.8)
     tvl1_case("tvl1_denoise", seed=31, w=48, h=40, niters=40)
     fusion_case("fusion_b7_decoupled", seed=41, dims=(20, 16, 12), bins=7, n_maps=3, w=48, h=40, iters=12,
                 interleaved=False)
@@ -195,6 +199,8 @@ def real_frame_case(name, n_src=4, factor=4, n_planes=64, win=5, znear=0.1, zfar
 
 
 CASES = {
+    "tgv_aniso": lambda: tgv_case("tgv_aniso", seed=23, w=56, h=44, n_src=3, niters=20, warps=2, start="depth",
+                                  beta=1.5, gamma=0.8),
     "tgv_sparse": lambda: tgv_sparse_case("tgv_sparse", seed=51, w=48, h=40, niters=60, frac=0.1),
     "real_frame": lambda: real_frame_case("real_frame"),
     "tgv_sparse_tensor": lambda: tgv_sparse_case("tgv_sparse_tensor", seed=52, w=37, h=29, niters=45, frac=0.25,

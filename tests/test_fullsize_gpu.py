@@ -1,0 +1,252 @@
+"""Parity at the sizes the bench reports, against the FP64 oracle.
+
+* the sweep of the bench (640x480, 8 views, 256 inverse-depth planes over
+  [0.4, 8] m, 9x9, compensated FP32 moments, BF16 cost volume, WTA) on the whole
+  frame: the FP64 oracle's mean NCC over the views per plane (the warp, box
+  means and calcNCC of kernels.cu:4-64,103-120,187-235 in double), its cost
+  1 - mean rounded to BF16 as the volume stores it, and its argmin;
+* TGV2 from that WTA depth to the energy tolerance of the bench (1e-4, checks
+  every 10 iterations, cap 500), against the FP64 oracle run from the same
+  depth for the GPU's iteration count (TGV2_kernels.cu:54-365,
+  planesweep.cpp:381-536);
+* TV-L1 histogram fusion of the bench (256^3 voxels over a 5 m cube, 40 maps of
+  640x480, 7 bins, 200 iterations; fusion.cu:5-70): the histograms against the
+  reference's arithmetic (the f32 oracle) bit for bit, and u, v against the
+  FP64 oracle's 200 iterations on those histograms.
+
+Each test records its measured errors; with MVS_PARITY_REPORT set, the
+session writes them to that JSON file.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+import mvs_b200 as M
+from mvs_b200 import scenes
+from test_sweep_gpu import bf16_round, run_sweep
+
+pytestmark = pytest.mark.gpu
+
+REPORT = {}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _write_report():
+    yield
+    path = os.environ.get("MVS_PARITY_REPORT")
+    if path and REPORT:
+        old = {}
+        if os.path.exists(path):
+            with open(path) as f:
+                old = json.load(f)
+        old.update(REPORT)
+        with open(path, "w") as f:
+            json.dump(old, f, indent=1)
+
+
+def q(a, p):
+    return float(np.quantile(a, p)) if a.size else 0.0
+
+
+def bf16_ulp(c):
+    """Spacing of BF16 values at c (c > 0): 2^(exponent - 7)."""
+    e = np.floor(np.log2(np.maximum(np.abs(c), 1e-30)))
+    return np.exp2(e - 7)
+
+
+BENCH_SEED = 2   # the bench's frame (bench.py SEED + rank 0)
+
+
+@pytest.fixture(scope="module")
+def c2_frame():
+    return scenes.config_full(seed=BENCH_SEED)
+
+
+@pytest.fixture(scope="module")
+def c2_sweep(cuda, c2_frame):
+    fr, planes, win = c2_frame
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    return run_sweep(cuda, fr.ref, fr.srcs, planes, win, K=fr.ref_cam.K_1based, Rref=fr.ref_cam.R,
+                     tref=fr.ref_cam.t, poses=poses, moments=M.MOMENTS_COMPENSATED, mode=M.SWEEP_AGGREGATED,
+                     zfar=8.0, cost=True)
+
+
+def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
+    """Labels identical to the FP64 oracle's on >= 99.9% of the pixels; every
+    other pixel within one plane, or a tie that BF16 storage cannot separate
+    (the FP64 costs of the two planes within one BF16 step).  The stored BF16
+    costs equal the FP64 cost rounded to BF16 except where the FP64 cost lies
+    within rounding distance of a BF16 boundary (at most one BF16 step off)."""
+    fr, planes, win = c2_frame
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    V = len(poses)
+    H64 = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, planes, precision="f64")
+    h, w = fr.ref.shape
+    gl = c2_sweep["label"][0]
+    gbits = c2_sweep["cost"]
+    n_same = n_near = n_tie = n_cost_same = n_far_not_tie = 0
+    max_cost_steps = 0.0
+    win_err = []
+    for y0 in range(0, h, 96):
+        y1 = min(h, y0 + 96)
+        c64 = np.maximum(1.0 - po.sweep_ncc_band(fr.ref, fr.srcs, H64, win, y0, y1) / V, 0.0)
+        cb = bf16_round(c64.astype(np.float32))
+        ol = np.argmin(cb, axis=0)
+        g = gl[y0:y1]
+        gc = (gbits[:, y0:y1].astype(np.uint32) << 16).view(np.float32)
+        n_cost_same += int(np.sum(gc == cb))
+        max_cost_steps = max(max_cost_steps, float(np.max(np.abs(gc - cb) / bf16_ulp(np.maximum(cb, 2.0 ** -20)))))
+        d = np.abs(g.astype(np.int64) - ol)
+        n_same += int(np.sum(d == 0))
+        n_near += int(np.sum(d <= 1))
+        far = d > 1
+        yy, xx = np.nonzero(far)
+        cg, co = c64[g[far], yy, xx], c64[ol[far], yy, xx]
+        tie = np.abs(cg - co) <= bf16_ulp(np.maximum(co, 2.0 ** -20))
+        n_tie += int(np.sum(tie))
+        n_far_not_tie += int(np.sum(~tie))
+        # the winning cost: the GPU's FP32 cost of its plane against the FP64 cost of that plane
+        yy, xx = np.nonzero(d == 0)
+        win_err.append(np.abs(gc[g[d == 0], yy, xx] - c64[g[d == 0], yy, xx]))
+    npx = h * w
+    win_err = np.concatenate(win_err)
+    rep = {"pixels": npx, "labels_identical": n_same / npx, "labels_within_one_plane": n_near / npx,
+           "labels_beyond_one_plane_bf16_ties": n_tie / npx, "labels_beyond_one_plane_not_ties": n_far_not_tie,
+           "cost_entries_identical_bf16": n_cost_same / (npx * len(planes)),
+           "cost_max_bf16_steps": max_cost_steps,
+           "winning_cost_abs_err_vs_fp64": {"p50": q(win_err, 0.5), "p99.9": q(win_err, 0.999),
+                                            "max": float(win_err.max())}}
+    REPORT["c2_sweep_aggregated_bf16_wta"] = rep
+    assert rep["labels_identical"] >= 0.999, rep
+    assert n_far_not_tie == 0, rep
+    assert max_cost_steps <= 1.0, rep
+
+
+def test_c3_fusion_vs_oracle(cuda):
+    """256^3 voxels, 40 depthmaps of 640x480 (1% noise, 2% outliers), 7 bins,
+    thr 0.05, 200 iterations, tau 0.1, lambda 0.5, sigma 1: the histograms equal
+    the reference's arithmetic bit for bit; u and v after 200 iterations are
+    within 1e-4 of the FP64 oracle's run on the same histograms."""
+    import torch
+    fi = scenes.fusion_sequence(BENCH_SEED + 100, 40, 640, 480)
+    dims, bins, iters = (256, 256, 256), 7, 200
+    Ks = np.stack([c.K for c in fi.cams]).astype(np.float32)
+    Rs = np.stack([c.R for c in fi.cams]).astype(np.float32)
+    ts = np.stack([c.t for c in fi.cams]).astype(np.float32)
+    vol = M.FusionVolume(dims, bins, fi.vol_min, fi.vol_max)
+    vol.histogram(torch.from_numpy(np.stack(fi.depths)).to(cuda), Ks, Rs, ts, 0.05)
+    vol.tvl1(iters, 0.1, 0.5, 1.0)
+    torch.cuda.synchronize()
+    r = vol.download()
+    vol.close()
+    o32 = po.Volume(bins, dims, fi.vol_min, fi.vol_max, precision="f32")
+    for m in range(len(fi.depths)):
+        o32.histogram(fi.depths[m], Ks[m], Rs[m], ts[m], 0.05)
+    hist_same = bool(np.array_equal(r["hist"], o32.hist))
+    # the votes an FP64 projection would move to another bin (voxels on a bin boundary)
+    o64 = po.Volume(bins, dims, fi.vol_min, fi.vol_max, precision="f64")
+    for m in range(len(fi.depths)):
+        o64.histogram(fi.depths[m], Ks[m], Rs[m], ts[m], 0.05)
+    moved = int(np.abs(o64.hist.astype(np.int64) - o32.hist).sum()) // 2
+    votes = int(o32.hist.sum(dtype=np.int64))
+    o64.hist[:] = o32.hist
+    o64.u[:] = 0
+    for _ in range(iters):
+        o64.update_u(0.1, 0.5)
+        o64.update_p(1.0)
+    eu = np.abs(r["u"] - o64.u)
+    ev = np.abs(r["v"] - o64.v)
+    rep = {"voxels": int(eu.size), "votes": votes, "histograms_identical_to_reference_arithmetic": hist_same,
+           "votes_moved_by_fp64_projection": moved,
+           "u_abs_err_vs_fp64": {"p99.9": q(eu, 0.999), "max": float(eu.max())},
+           "v_abs_err_vs_fp64": {"p99.9": q(ev, 0.999), "max": float(ev.max())},
+           "surface_voxels": int(np.sum((r["u"] > -1) & (r["u"] < 0)))}
+    REPORT["c3_fusion"] = rep
+    assert hist_same, rep
+    assert rep["u_abs_err_vs_fp64"]["p99.9"] <= 1e-4 and rep["u_abs_err_vs_fp64"]["max"] <= 1e-3, rep
+
+
+def tgv_rel_errors(u, uo):
+    rel = np.abs(u.astype(np.float64) - uo) / np.abs(uo)
+    return {"max": float(rel.max()), "p99.9": q(rel, 0.999),
+            "l2": float(np.linalg.norm(u.astype(np.float64) - uo) / np.linalg.norm(uo))}
+
+
+def test_c2_tgv2_to_tolerance_vs_fp64_oracle(cuda, c2_frame, c2_sweep):
+    """TGV2 of the bench (lambda 0.5, alpha0 2, alpha1 1.5, tau 0.02, sigma 1,
+    one linearisation at the WTA depth, tolerance 1e-4 over a 5-check window,
+    checks every 10 iterations, cap 500) against the FP64 oracle from the same
+    WTA depth with the same rule: the same stopping iteration, and at it the
+    depth and the energy within 1e-4 relative."""
+    import torch
+    from mvs_b200 import hostmath as hm
+    fr, planes, win = c2_frame
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    u0 = c2_sweep["depth"]
+    Kf = np.float32(K1)
+    relf = [hm.relative_f32(fr.ref_cam.R, fr.ref_cam.t, c.R, c.t) for c in fr.src_cams]
+    prm = M.tgv2_params(niters=500, warps=1, tol=1e-4, check_every=10)
+    h, w = u0.shape
+    u = torch.from_numpy(np.ascontiguousarray(u0)).to(cuda)
+    tws = torch.empty(M.tgv2_workspace_bytes(w, h, len(poses)) // 8 + 1, dtype=torch.int64, device=cuda)
+    it, e = M.tgv2_run(torch.from_numpy(fr.ref).to(cuda), torch.from_numpy(np.stack(fr.srcs)).to(cuda),
+                       Kf.reshape(9), hm.inv3_f32(Kf).reshape(9), np.stack([r[0].reshape(9) for r in relf]),
+                       np.stack([r[1] for r in relf]), prm, u, u_from_input=True, workspace=tws)
+    torch.cuda.synchronize()
+    ug = u.cpu().numpy()
+    uo, ito, eo = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=500, warps=1, u_init=u0,
+                          precision="f64", tol=1e-4, check_every=10)
+    if ito != it:   # compare at the GPU's count
+        uo, _, eo = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=it, warps=1, u_init=u0,
+                            precision="f64", tol=1e-30, check_every=10)
+    eo_it = eo[it // 10 - 1]
+    rep = {"iterations_gpu": it, "iterations_fp64": ito, "energy_gpu": e, "energy_fp64": eo_it,
+           "energy_rel_err": abs(e - eo_it) / abs(eo_it), "depth_rel_err": tgv_rel_errors(ug, uo)}
+    REPORT["c2_tgv2_plain"] = rep
+    assert abs(it - ito) <= 10, rep
+    assert rep["energy_rel_err"] <= 1e-4, rep
+    assert rep["depth_rel_err"]["p99.9"] <= 1e-4 and rep["depth_rel_err"]["l2"] <= 1e-4, rep
+
+
+def test_c2_tgv2_warm_start_vs_fp64_oracle(cuda):
+    """The warm-started run of the bench on a held-out frame (seed 920000: the
+    network's prediction from the WTA depth, matching cost and image; the data
+    term linearised at the WTA depth; tau 0.008, sigma 2.5; the one-step dual
+    start; the same tolerance, window and cap) against the FP64 oracle replaying
+    the same run from the same prediction: the depth within 1e-4 relative."""
+    import torch
+    from mvs_b200 import warmstart as WS
+    cfg = WS.FrameConfig()
+    params, norm, _ = WS.load_weights()
+    pipe = WS.Pipeline(cfg, cuda)
+    fr = scenes.GpuRenderer(cuda).frame(920000, cfg.width, cfg.height, cfg.K, cfg.n_src, baseline=cfg.baseline)
+    cams = pipe.cams(fr)
+    d, c = pipe.sweep(fr, cams)
+    wta = d.clone()
+    ws = WS.WarmStart(cfg, params, norm, cuda)
+    pu, pv = ws.predict(wta[None], c[None], fr.ref[None])
+    u0p, v0p = pu.reshape(cfg.height, cfg.width).cpu().numpy(), pv.reshape(2, cfg.height, cfg.width).cpu().numpy()
+    u = pu.reshape(cfg.height, cfg.width).clone()
+    v = pv.reshape(2, cfg.height, cfg.width).clone()
+    prm = WS.tgv_params(tau=WS.WARM_TAU, sigma=WS.WARM_SIGMA)
+    it, e = pipe.tgv(fr, wta, u, v, prm, dual_sigma=WS.WARM_DUAL_SIGMA, dual_sigma_r=WS.WARM_DUAL_SIGMA_R, cams=cams)
+    torch.cuda.synchronize()
+    ug = u.cpu().numpy()
+    poses = [(cm.R, cm.t) for cm in fr.src_cams]
+    ref, srcs = fr.ref.cpu().numpy(), list(fr.srcs.cpu().numpy())
+    args = (ref, srcs, fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, poses, wta.cpu().numpy(), u0p, v0p,
+            WS.WARM_DUAL_SIGMA, WS.WARM_DUAL_SIGMA_R)
+    uo, ito, eo = po.tgv2_warm(*args, max_iters=500, tau=WS.WARM_TAU, sigma=WS.WARM_SIGMA, tol=1e-4)
+    if ito != it:
+        uo, _, eo = po.tgv2_warm(*args, max_iters=it, tau=WS.WARM_TAU, sigma=WS.WARM_SIGMA, tol=1e-30)
+    eo_it = eo[it // 10 - 1]
+    rep = {"iterations_gpu": it, "iterations_fp64": ito, "energy_gpu": e, "energy_fp64": eo_it,
+           "energy_rel_err": abs(e - eo_it) / abs(eo_it), "depth_rel_err": tgv_rel_errors(ug, uo)}
+    REPORT["c2_tgv2_warm"] = rep
+    assert abs(it - ito) <= 10, rep
+    assert rep["energy_rel_err"] <= 1e-4, rep
+    assert rep["depth_rel_err"]["p99.9"] <= 1e-4 and rep["depth_rel_err"]["l2"] <= 1e-4, rep

@@ -47,6 +47,30 @@ def test_sweep_f64_labels_vs_golden(golden, name):
     assert np.all(np.abs(o["best"][far] - g["best"][far]) < 1e-4)
 
 
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_sweep_ncc_band_equals_full_frame_rows(precision):
+    """The row-band cost used for full-size checks equals the same rows of the
+    full-frame per-view NCC summed over views, bit for bit: a band at the top
+    (mirrored rows above the frame), one inside and one at the bottom."""
+    fr, planes, win = scenes.config_tiny(seed=11, width=37, height=29, n_src=3, n_planes=5, win=7)
+    pz = [(c.R, c.t) for c in fr.src_cams]
+    H = po.homographies(fr.ref_cam.K_1based, fr.ref_cam.R, fr.ref_cam.t, pz, planes, precision=precision)
+    L = po.oracle_lib()
+    dt = np.float32 if precision == "f32" else np.float64
+    P = po._fp if precision == "f32" else po._dp
+    h, w = fr.ref.shape
+    full = np.zeros((len(planes), h, w), dt)
+    for p in range(len(planes)):
+        for v in range(len(pz)):
+            buf = np.zeros((h, w), dt)
+            getattr(L, f"orc_sweep_ncc_{precision}")(w, h, po._fp(po._f32(fr.ref)), po._fp(po._f32(fr.srcs[v])),
+                                                     P(np.ascontiguousarray(H[v, p], dt)), win, 1e-4, P(buf))
+            full[p] = (full[p] + buf).astype(dt)
+    for y0, y1 in [(0, 6), (9, 20), (25, 29)]:
+        band = po.sweep_ncc_band(fr.ref, fr.srcs, H, win, y0, y1, precision=precision)
+        np.testing.assert_array_equal(band, full[:, y0:y1])
+
+
 def test_reference_plane_loop(golden):
     g = golden("sweep_refloop_w7")
     np.testing.assert_array_equal(po.plane_list(float(g["znear"]), float(g["zfar"]), 24), g["planes"])
@@ -55,15 +79,17 @@ def test_reference_plane_loop(golden):
     assert len(po.plane_list(0.1, 1.0, 200)) == 199
 
 
-@pytest.mark.parametrize("name", ["tgv_from_one", "tgv_from_depth"])
+@pytest.mark.parametrize("name", ["tgv_from_one", "tgv_from_depth", "tgv_aniso"])
 def test_tgv2_f32_bit_exact_vs_golden(golden, name):
+    """tgv_aniso: beta = 1.5, gamma = 0.8, the anisotropic tensor on."""
     g = golden(name)
     u0 = None if str(g["start"]) == "one" else g["depth_gt"]
+    bg = dict(beta=float(g["beta"]), gamma=float(g["gamma"])) if "beta" in g else {}
     u, n, _ = po.tgv2(g["ref"], list(g["srcs"]), g["K"], g["Rref"], g["tref"], poses(g), niters=int(g["niters"]),
-                      warps=int(g["warps"]), u_init=u0, precision="f32")
+                      warps=int(g["warps"]), u_init=u0, precision="f32", **bg)
     np.testing.assert_array_equal(u, g["u"])
     u64, _, _ = po.tgv2(g["ref"], list(g["srcs"]), g["K"], g["Rref"], g["tref"], poses(g),
-                        niters=int(g["niters"]), warps=int(g["warps"]), u_init=u0, precision="f64")
+                        niters=int(g["niters"]), warps=int(g["warps"]), u_init=u0, precision="f64", **bg)
     assert np.max(np.abs(u64 - g["u"]) / np.abs(u64)) < 1e-4
 
 
@@ -160,6 +186,30 @@ needs_ref = pytest.mark.skipif(po.ref_lib() is None, reason="reference-on-CPU li
 
 
 @needs_ref
+@pytest.mark.parametrize("bins", [3, 7, 10])
+def test_fp64_fusion_u_median_equals_sorted_selection(bins):
+    """The FP64 oracle's U step (merge selection) against a plain sort: the
+    median (rank N) of the bin centres, u and u + tau lambda W_j, each raised
+    to the lowest centre as the reference's insertion leaves it."""
+    rng = np.random.default_rng(bins)
+    dims = (9, 7, 5)
+    n = 9 * 7 * 5
+    o = po.Volume(bins, dims, [0, 0, 0], [1, 1, 1], precision="f64")
+    o.hist[:] = rng.integers(0, 9, o.hist.shape)
+    o.hist[:, :10] = 0
+    u0 = rng.uniform(-2.5, 2.5, n)
+    o.u[:] = u0
+    tau, lam = 0.1, 0.5
+    o.update_u(tau, lam)   # p = 0: the divergence term vanishes
+    c = po.bin_centers(bins).astype(np.float64)
+    h = o.hist.astype(np.int64)
+    for i in range(n):
+        W = [-h[:j, i].sum() + h[j:, i].sum() for j in range(1, bins + 1)]
+        vals = np.concatenate([c, [u0[i]], u0[i] + tau * lam * np.asarray(W, np.float64)])
+        vals = np.maximum(vals, c[0])
+        assert o.u[i] == np.sort(vals)[bins], i
+
+
 def test_live_sweep_vs_reference():
     fr, planes, win = scenes.config_tiny(seed=101, width=72, height=50, n_src=3, n_planes=20, win=9)
     p = [(c.R, c.t) for c in fr.src_cams]

@@ -50,6 +50,44 @@ def test_tgv2_bit_exact_vs_reference(cuda, golden, name):
     np.testing.assert_array_equal(u, g["u"])
 
 
+def test_tgv2_anisotropic_tensor_vs_reference(cuda, golden):
+    """beta = 1.5, gamma = 0.8: the anisotropic diffusion tensor
+    (TGV2_kernels.cu:257-298) weights the P step and the divergence of the U
+    step (:300-365).  The tensor is computed with CUDA's expf/powf, the
+    reference run on the CPU with the host's: a one-ulp difference of a tensor
+    entry moves the depth by far less than 1e-5 relative, so the bar is 1e-5
+    (the rest of the arithmetic is the reference's)."""
+    g = golden("tgv_aniso")
+    K9, iK9, Rs, ts = tgv_inputs(g)
+    p = M.tgv2_params(niters=int(g["niters"]), warps=int(g["warps"]), beta=float(g["beta"]), gamma=float(g["gamma"]))
+    u, it, _ = run_tgv(cuda, g["ref"], list(g["srcs"]), K9, iK9, Rs, ts, p, g["depth_gt"])
+    assert it == int(g["niters"]) * int(g["warps"])
+    rel = np.abs(u.astype(np.float64) - g["u"]) / np.abs(g["u"])
+    assert rel.max() <= 1e-5, rel.max()
+    # the tensor is really on: the isotropic run differs
+    u_iso, _, _ = run_tgv(cuda, g["ref"], list(g["srcs"]), K9, iK9, Rs, ts,
+                          M.tgv2_params(niters=int(g["niters"]), warps=int(g["warps"])), g["depth_gt"])
+    assert np.max(np.abs(u_iso - g["u"]) / np.abs(g["u"])) > 1e-4
+
+
+def test_tgv2_anisotropic_tensor_through_handle(cuda, golden):
+    """The same run through the PlaneSweep handle (PlaneSweep::TGV with beta,
+    gamma: planesweep.cpp:381-536), host images in and out."""
+    g = golden("tgv_aniso")
+    ps = M.PlaneSweep()
+    ps.setK(g["K"])
+    ps.setNumberofImages(len(g["srcs"]))
+    ps.set_reference(g["ref"], g["Rref"], g["tref"])
+    ps.set_sources(g["srcs"], g["Rsrc"], g["tsrc"])
+    p = M.tgv2_params(niters=int(g["niters"]), warps=int(g["warps"]), beta=float(g["beta"]), gamma=float(g["gamma"]))
+    it, _ = ps.TGVext(p, start=2, u_init=g["depth_gt"])
+    assert it == int(g["niters"]) * int(g["warps"])
+    u = ps.getDepthmapTGV()
+    ps.close()
+    rel = np.abs(u.astype(np.float64) - g["u"]) / np.abs(g["u"])
+    assert rel.max() <= 1e-5, rel.max()
+
+
 def test_tgv2_tolerance_vs_fp64_oracle(cuda):
     """TGV2 from a noisy start with an energy tolerance: the FP64 oracle stops within one check
     of the GPU, and at the GPU's iteration count the depth and the energy agree within 1e-4
