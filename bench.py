@@ -377,13 +377,15 @@ def run_batched(args, dev, stream, flush, rank):
     kinds = {}
     for sp in specs:
         kinds[sp.kind] = kinds.get(sp.kind, 0) + 1
-    ppc, ctas, order = b.tuning
+    ppc, ctas, order, tile_step = b.tuning
     out = {"frames": len(frames), "mix": kinds, "evals_per_batch": evals,
            "value": evals * dist.world()[1] / (batch_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_batch": batch_ms,
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max()), "samples": int(lat.size)},
            "tuning": {"planes_per_chunk": ppc, "ctas_per_sm": ctas,
-                      "order": ["frame", "largest_first", "interleaved"][order]},
+                      "order": ["frame", "largest_first", "interleaved"][order],
+                      "tile": f"32 rows x (64 or 56 for windows above 9x9) - {8 * tile_step} columns",
+                      "tile_step": tile_step},
            "autotune_s": tune_s, "work_items": b.work_items,
            "sequential_single_frame_ms": statistics.mean(seq), "launches_per_batch": 4,
            "planes": [sp.n_planes for sp in specs], "windows": [sp.window for sp in specs]}

@@ -427,6 +427,11 @@ typedef struct mvs_batch_tuning {
     int32_t planes_per_chunk;   /* 0: whole plane range per item */
     int32_t ctas_per_sm;        /* persistent CTAs per SM (1..3) */
     int32_t order;              /* MVS_BATCH_ORDER_* */
+    int32_t tile_step;          /* tile shape: 32 rows x (64 - 8 tile_step) columns for windows up to
+                                   9x9, x (56 - 8 tile_step) above; 0 or 1.  The compensated
+                                   moments shift each tile's sums by the tile's reference mean, so
+                                   two tile shapes agree to rounding, not bit for bit: pass an
+                                   explicit tuning for bit-reproducible batches. */
 } mvs_batch_tuning;
 
 typedef struct mvs_batch mvs_batch;

@@ -356,12 +356,15 @@ public:
     Rectangle3D volume() const { return vol_; }
     bool valid() const { return f_ != 0; }
     mvs_fusion *handle() const { return f_; }
+    /* Resize (fusion.h:298-306): new storage of w x h x d voxels, managed by
+     * this object from now on; the bounding volume is kept. */
     void Resize(size_t w, size_t h, size_t d)
     {
         if (own_) mvs_fusion_destroy(f_);
-        *this = fusionData();
-        fusionData t(w, h, d, vol_.a, vol_.b);
-        f_ = t.f_; own_ = true; t.own_ = false;
+        f_ = 0;
+        const float fa[3] = {vol_.a.x, vol_.a.y, vol_.a.z}, fb[3] = {vol_.b.x, vol_.b.y, vol_.b.z};
+        if (mvs_fusion_create((int)w, (int)h, (int)d, N, fa, fb, &f_) != MVS_OK) f_ = 0;
+        own_ = true;
         w_ = w; h_ = h; d_ = d;
     }
     void setVolume(Rectangle3D &vol)

@@ -8,10 +8,10 @@
 // 1 - mean NCC over views, winner-take-all) is computed, with the moments the
 // caller picks.
 //
-// The work list's plane chunk size, the number of persistent CTAs per SM and
-// the item order are chosen by an autotuner that times each candidate on the
-// batch itself; its choice is cached per batch shape (the only global mutable
-// state of the library).
+// The work list's plane chunk size, the number of persistent CTAs per SM, the
+// item order and the tile shape are chosen by an autotuner that times each
+// candidate on the batch itself; its choice is cached per batch shape (the
+// only global mutable state of the library).
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -21,11 +21,11 @@
 #include "common.cuh"
 
 namespace mvs {
-int sweep_tile_width(int win);
+int sweep_tile_width(int win, int tws);
 int sweep_tile_height();
 int sweep_batch_launch(const BatchFrameDev *frames, const uint4 *items, int n_items, unsigned int *next,
                        unsigned long long *t_start, const BatchCamDev *cams, const int *hom_offsets, int n_frames,
-                       int n_hom, int moments, int ctas, void *stream);
+                       int n_hom, int moments, int ctas, int tws, void *stream);
 }  // namespace mvs
 
 using namespace mvs;
@@ -54,6 +54,7 @@ struct mvs_batch {
 
 namespace {
 
+constexpr int kBatchTileSteps = 2;   // tile shapes the batched sweep is compiled for
 std::mutex g_tune_lock;
 std::map<std::string, mvs_batch_tuning> g_tune_cache;
 
@@ -118,6 +119,9 @@ int build_items(mvs_batch *b, const mvs_batch_tuning &t)
     for (int i = 0; i < b->n; ++i) {
         BatchFrameDev &d = b->fdev[i];
         const mvs_batch_frame &f = b->frames[i];
+        d.tile_w = sweep_tile_width(f.window, t.tile_step);
+        d.tiles_x = ceil_div(f.width, d.tile_w);
+        d.n_tiles = d.tiles_x * ceil_div(f.height, sweep_tile_height());
         const int ppc = t.planes_per_chunk > 0 ? std::min(t.planes_per_chunk, f.n_planes) : f.n_planes;
         d.planes_per_chunk = ppc;
         d.n_chunks = ceil_div(f.n_planes, ppc);
@@ -177,7 +181,7 @@ int capture(mvs_batch *b, const mvs_batch_tuning &t)
     cudaGraph_t g = nullptr;
     MVS_TRY_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
     int rc = sweep_batch_launch(b->d_frames, b->d_items, b->n_items, b->d_next, b->d_t0, b->d_cams, b->d_hom_off, b->n,
-                                b->n_hom, b->moments, ctas, b->cap);
+                                b->n_hom, b->moments, ctas, t.tile_step, b->cap);
     cudaError_t e = cudaStreamEndCapture(b->cap, &g);
     if (rc) {
         if (g) cudaGraphDestroy(g);
@@ -192,6 +196,9 @@ int capture(mvs_batch *b, const mvs_batch_tuning &t)
 
 int apply(mvs_batch *b, const mvs_batch_tuning &t)
 {
+    if (t.tile_step < 0 || t.tile_step > kBatchTileSteps - 1)
+        return set_error(MVS_ERR_ARG, "tile_step %d (0..%d)", t.tile_step, kBatchTileSteps - 1);
+    if (t.ctas_per_sm < 1 || t.ctas_per_sm > 3) return set_error(MVS_ERR_ARG, "ctas_per_sm %d (1..3)", t.ctas_per_sm);
     int rc = build_items(b, t);
     if (rc) return rc;
     rc = capture(b, t);
@@ -216,28 +223,40 @@ int run_timed(mvs_batch *b, cudaStream_t st, float *ms)
     return MVS_OK;
 }
 
+// Search: plane chunk x CTAs per SM x item order on the widest tile, then the
+// best of those on the narrower tile (72 candidates would double the tuning
+// time; the tile shape interacts mostly with the chunk size and CTA count).
 int autotune(mvs_batch *b, mvs_batch_tuning *best)
 {
     const int chunks[] = {16, 32, 64, 0};
     const int ctas[] = {1, 2, 3};
     const int orders[] = {MVS_BATCH_ORDER_FRAME, MVS_BATCH_ORDER_LARGEST_FIRST, MVS_BATCH_ORDER_INTERLEAVED};
     float best_ms = 1e30f;
+    auto trial = [&](const mvs_batch_tuning &t) -> int {
+        int rc = apply(b, t);
+        if (rc) return rc;
+        float ms = 0.f, m2 = 0.f;
+        if ((rc = run_timed(b, b->cap, &ms))) return rc;   // warm-up
+        if ((rc = run_timed(b, b->cap, &ms))) return rc;
+        if ((rc = run_timed(b, b->cap, &m2))) return rc;
+        ms = std::min(ms, m2);
+        if (ms < best_ms) {
+            best_ms = ms;
+            *best = t;
+        }
+        return MVS_OK;
+    };
     for (int c : chunks)
         for (int k : ctas)
             for (int o : orders) {
-                mvs_batch_tuning t{c, k, o};
-                int rc = apply(b, t);
-                if (rc) return rc;
-                float ms = 0.f, m2 = 0.f;
-                if ((rc = run_timed(b, b->cap, &ms))) return rc;   // warm-up
-                if ((rc = run_timed(b, b->cap, &ms))) return rc;
-                if ((rc = run_timed(b, b->cap, &m2))) return rc;
-                ms = std::min(ms, m2);
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    *best = t;
-                }
+                mvs_batch_tuning t{c, k, o, 0};
+                if (int rc = trial(t)) return rc;
             }
+    // the narrower tile with the chunk sizes and CTA counts around the best so far
+    const mvs_batch_tuning w = *best;
+    for (int c : chunks)
+        for (int k : ctas)
+            if (int rc = trial(mvs_batch_tuning{c, k, w.order, 1})) return rc;
     return MVS_OK;
 }
 
@@ -274,7 +293,9 @@ int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, 
     std::vector<size_t> o_H(n), o_wta(n), o_tiles(n), o_fl(n), o_quad(n);
     for (int i = 0; i < n; ++i) {
         const mvs_batch_frame &f = frames[i];
-        const int tw = sweep_tile_width(f.window), th = sweep_tile_height();
+        // tile counts of the widest tile here; build_items sets those of the tuning
+        const int tw = sweep_tile_width(f.window, 0), th = sweep_tile_height();
+        const int tiles_max = ceil_div(f.width, sweep_tile_width(f.window, kBatchTileSteps - 1)) * ceil_div(f.height, th);
         BatchFrameDev &d = b->fdev[i];
         d.w = f.width;
         d.h = f.height;
@@ -289,7 +310,7 @@ int mvs_batch_create(mvs_batch **out, const mvs_batch_frame *frames, int32_t n, 
         b->hom_off[i + 1] = b->hom_off[i] + f.n_views * f.n_planes;
         o_H[i] = take((size_t)f.n_views * f.n_planes * 9 * sizeof(float));
         o_wta[i] = take((size_t)f.width * f.height * 8);
-        o_tiles[i] = take((size_t)d.n_tiles * sizeof(unsigned));
+        o_tiles[i] = take((size_t)tiles_max * sizeof(unsigned));
         o_fl[i] = take(sizeof(unsigned));
         // 2x2 source neighbourhoods, rebuilt from the sources at every launch
         o_quad[i] = take((size_t)f.width * f.height * f.n_views * sizeof(float4));

@@ -52,10 +52,12 @@ constexpr int RHMAX = TH + 15;   // region rows of the largest window (15), plus
 constexpr int CSP = 76;
 constexpr int STRIP = 11;     // output rows per pass-A1 thread (the last strip has 10)
 
-template <int WIN>
+// TWS narrows the tile by 8 output columns per step (the batched sweep's
+// autotuner picks it; every other launch uses the widest tile, TWS = 0).
+template <int WIN, int TWS = 0>
 struct Geo {
     static constexpr int R = WIN / 2;
-    static constexpr int TW = ((RWMAX - 2 * R) / 8) * 8;  // output columns: 64 up to 9x9, 56 above
+    static constexpr int TW = ((RWMAX - 2 * R) / 8 - TWS) * 8;  // output columns: 64 up to 9x9, 56 above
     static constexpr int RUN = TW / 8;                     // outputs per thread in pass B
     static constexpr int RW = TW + 2 * R;                  // region columns used
     static constexpr int RH = TH + 2 * R;                  // region rows
@@ -127,10 +129,10 @@ __device__ __forceinline__ void load_run(const float *row, float *v)
     }
 }
 
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ void row_sums(const float (*CSq)[CSP], float *out)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     constexpr int NV = G::RUN + 2 * G::R;
     static_assert(G::RUN % 4 != 0 || 7 * G::RUN + 4 * ((NV + 3) / 4) <= CSP, "run loads stay inside a row");
     float v[NV];
@@ -161,20 +163,20 @@ __device__ __forceinline__ void row_sums(const float (*CSq)[CSP], float *out)
 // Sxx: about 3 n eps per addition, with WIN + 2 (STRIP - 1) additions along
 // a column strip and WIN + 2 (RUN - 1) along a row run.  Windows at or below
 // it count as flat.
-template <int WIN>
+template <int WIN, int TWS = 0>
 __device__ __forceinline__ constexpr float flat_kappa()
 {
-    return 3.f * (float)(WIN * WIN) * (float)(2 * WIN + 2 * (STRIP - 1) + 2 * (Geo<WIN>::RUN - 1)) * 5.9604645e-8f;
+    return 3.f * (float)(WIN * WIN) * (float)(2 * WIN + 2 * (STRIP - 1) + 2 * (Geo<WIN, TWS>::RUN - 1)) * 5.9604645e-8f;
 }
 
 // Reference moments of the tile, once per CTA: in REFERENCE mode the mean and
 // the naive std (calculate_STD_kernel, kernels.cu:103-120) of the reference
 // window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2 (0 if flat).
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float (*RM)[CSP],
                             float (*RS)[CSP])
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     if (threadIdx.x < G::COLT) {
         const int c = threadIdx.x % G::RW, s = threadIdx.x / G::RW;
         const int r0 = STRIP * s;
@@ -204,8 +206,8 @@ __device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], floa
     }
     __syncthreads();
     float m[G::RUN], q[G::RUN];
-    row_sums<WIN, MOM>(CS[0], m);
-    row_sums<WIN, MOM>(CS[1], q);
+    row_sums<WIN, MOM, TWS>(CS[0], m);
+    row_sums<WIN, MOM, TWS>(CS[1], q);
     const int y = b_row(), x = b_seg() * G::RUN;
 #pragma unroll
     for (int j = 0; j < G::RUN; ++j) {
@@ -216,13 +218,13 @@ __device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], floa
         } else {
             const float v = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
             RM[y][x + j] = m[j];
-            RS[y][x + j] = v > flat_kappa<WIN>() * q[j] ? v : 0.f;
+            RS[y][x + j] = v > flat_kappa<WIN, TWS>() * q[j] ? v : 0.f;
         }
     }
     __syncthreads();
 }
 
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm, float rs, float st)
 {
     if (MOM == MVS_MOMENTS_REFERENCE) {
@@ -235,7 +237,7 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
         const float vx = fmaf(-s1, s1, n * s2);         // n^2 var_w
         const float cv = fmaf(-s1, rm, n * s12);        // n^2 cov
         const float thr = st * n;                        // std >= st  <=>  n^2 var >= (st n)^2
-        if (!(vx >= thr * thr) || !(rs >= thr * thr) || !(vx > flat_kappa<WIN>() * s2)) return 0.f;
+        if (!(vx >= thr * thr) || !(rs >= thr * thr) || !(vx > flat_kappa<WIN, TWS>() * s2)) return 0.f;
         return cv * rsqrtf(vx * rs);
     }
 }
@@ -243,11 +245,11 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
 // The NCC of a run of RUN outputs against the reference moments, which are
 // read in groups of four (one 16-byte load each when RUN is a multiple of 4),
 // so at most four of them are live at a time.
-template <int WIN, int MOM, typename F>
+template <int WIN, int MOM, int TWS, typename F>
 __device__ __forceinline__ void ncc_run(const float *s1, const float *s2, const float *s12, const float *rmrow,
                                         const float *rsrow, float st, F &&use)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
 #pragma unroll
     for (int j0 = 0; j0 < G::RUN; j0 += 4) {
         float rm[4], rs[4];
@@ -265,7 +267,7 @@ __device__ __forceinline__ void ncc_run(const float *s1, const float *s2, const 
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (j0 + i < G::RUN) use(j0 + i, ncc_of<WIN, MOM>(s1[j0 + i], s2[j0 + i], s12[j0 + i], rm[i], rs[i], st));
+            if (j0 + i < G::RUN) use(j0 + i, ncc_of<WIN, MOM, TWS>(s1[j0 + i], s2[j0 + i], s12[j0 + i], rm[i], rs[i], st));
     }
 }
 
@@ -277,11 +279,11 @@ struct __align__(16) Smem {
     float red[THREADS / 32];
 };
 
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ void load_ref_region(Smem &S, const float *__restrict__ ref, int w, int h, int x0,
                                                 int y0)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
         const int ry = i / RWMAX, rx = i % RWMAX;
         if (rx >= G::RW) continue;
@@ -291,10 +293,10 @@ __device__ __forceinline__ void load_ref_region(Smem &S, const float *__restrict
 
 // Shift of the compensated sums: the mean of the tile's reference region
 // (block reduction; every thread returns the same value).  0 in REFERENCE mode.
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ float tile_shift(Smem &S)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     if (MOM == MVS_MOMENTS_REFERENCE) return 0.f;
     float acc = 0.f;
     for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
@@ -390,12 +392,12 @@ constexpr int kFloorMagicBits = 0x4B400000;
 // the source's 2x2 neighbourhoods (difference form in COMPENSATED), else the
 // four samples are gathered from `src`.  COMPENSATED stores the samples
 // shifted by `shift`.
-template <int WIN, int MOM, bool QUAD>
+template <int WIN, int MOM, bool QUAD, int TWS = 0>
 __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src,
                                              const float4 *__restrict__ quad, int w, int h, const float *Hm, float X,
                                              const float *Yc, float shift)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     constexpr int CELLS = G::A0ROWS;
     constexpr int BATCH = 4;
     if (threadIdx.x >= G::COLT) return;
@@ -492,11 +494,11 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
 // pass A1 with the reference column read from shared memory: thread (c, s)
 // forms the column sums of w, w^2 and ref*w for output rows [11 s, 11 s + 11)
 // (COMPENSATED: Wt and Rf hold shifted values already)
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ void pass_a1_rows(const float (*Wt)[RWMAX], float (*CS)[TH][CSP],
                                              const float (*Rf)[RWMAX])
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     if (threadIdx.x >= G::COLT) return;
     const int c = threadIdx.x % G::RW, s = threadIdx.x / G::RW;
     const int r0 = STRIP * s;
@@ -551,25 +553,25 @@ __device__ __forceinline__ void pass_a1_rows(const float (*Wt)[RWMAX], float (*C
 }
 
 // One CTA's work: tile (tx, ty) of the frame, planes of `chunk`.
-template <int WIN, int MOM>
+template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, int tx, int ty, int chunk)
 {
-    using G = Geo<WIN>;
+    using G = Geo<WIN, TWS>;
     Smem &S = A.S;
     const int x0 = tx * G::TW, y0 = ty * TH;
     const int w = a.w, h = a.h;
     const size_t n = (size_t)w * h;
 
-    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    load_ref_region<WIN, MOM, TWS>(S, a.ref, w, h, x0, y0);
     for (int i = threadIdx.x; i < G::RH; i += THREADS) A.Yc[i] = (float)(mirror_idx(y0 - G::R + i, h) + 1);
     __syncthreads();
-    const float shift = tile_shift<WIN, MOM>(S);
+    const float shift = tile_shift<WIN, MOM, TWS>(S);
     for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
         const int ry = i / RWMAX, rx = i % RWMAX;
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    ref_moments<WIN, MOM, TWS>(S.Wt, S.CS, shift, A.RM, A.RS);
     const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
 
     const int ly = b_row(), lx = b_seg() * G::RUN;
@@ -604,19 +606,19 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             float hn = 0.f;
             if (threadIdx.x < 9 && np < p1) hn = ldg(a.H + ((size_t)nv * a.P + np) * 9 + threadIdx.x);
             if (a.quad)
-                pass_a0_rows<WIN, MOM, true>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc, sh);
+                pass_a0_rows<WIN, MOM, true, TWS>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc, sh);
             else
-                pass_a0_rows<WIN, MOM, false>(S.Wt, a.srcs + (size_t)view * n, nullptr, w, h, Hm, Xcol, A.Yc, sh);
+                pass_a0_rows<WIN, MOM, false, TWS>(S.Wt, a.srcs + (size_t)view * n, nullptr, w, h, Hm, Xcol, A.Yc, sh);
             if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
             hb ^= 1;
             __syncthreads();
-            pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
+            pass_a1_rows<WIN, MOM, TWS>(S.Wt, S.CS, A.Rf);
             __syncthreads();
             float s1[G::RUN], s2[G::RUN], s12[G::RUN];
-            row_sums<WIN, MOM>(S.CS[0], s1);
-            row_sums<WIN, MOM>(S.CS[1], s2);
-            row_sums<WIN, MOM>(S.CS[2], s12);
-            ncc_run<WIN, MOM>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh,
+            row_sums<WIN, MOM, TWS>(S.CS[0], s1);
+            row_sums<WIN, MOM, TWS>(S.CS[1], s2);
+            row_sums<WIN, MOM, TWS>(S.CS[2], s12);
+            ncc_run<WIN, MOM, TWS>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh,
                               [&](int j, float c) { acc[j] += c; });
         }
         uint16_t cb[G::RUN];
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         row_sums<WIN, MOM>(S.CS[0], s1);
         row_sums<WIN, MOM>(S.CS[1], s2);
         row_sums<WIN, MOM>(S.CS[2], s12);
-        ncc_run<WIN, MOM>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh, [&](int j, float c) {
+        ncc_run<WIN, MOM, 0>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh, [&](int j, float c) {
             if (c > best[j]) {
                 best[j] = c;
                 lab[j] = p;
@@ -920,7 +922,7 @@ __global__ void batch_start_kernel(unsigned int *next, unsigned long long *t_sta
     *t_start = global_timer_ns();
 }
 
-template <int MOM>
+template <int MOM, int TWS>
 __global__ void __launch_bounds__(THREADS, 3) sweep_batch_kernel(const BatchFrameDev *__restrict__ frames,
                                                                   const uint4 *__restrict__ items, int n_items,
                                                                   unsigned int *next)
@@ -953,13 +955,13 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_batch_kernel(const BatchFram
         a.quad = f.quad;
         const int tx = (int)item.y % f.tiles_x, ty = (int)item.y / f.tiles_x;
         switch (f.win) {
-        case 3: aggregated_tile<3, MOM>(S, a, tx, ty, item.z); break;
-        case 5: aggregated_tile<5, MOM>(S, a, tx, ty, item.z); break;
-        case 7: aggregated_tile<7, MOM>(S, a, tx, ty, item.z); break;
-        case 9: aggregated_tile<9, MOM>(S, a, tx, ty, item.z); break;
-        case 11: aggregated_tile<11, MOM>(S, a, tx, ty, item.z); break;
-        case 13: aggregated_tile<13, MOM>(S, a, tx, ty, item.z); break;
-        default: aggregated_tile<15, MOM>(S, a, tx, ty, item.z); break;
+        case 3: aggregated_tile<3, MOM, TWS>(S, a, tx, ty, item.z); break;
+        case 5: aggregated_tile<5, MOM, TWS>(S, a, tx, ty, item.z); break;
+        case 7: aggregated_tile<7, MOM, TWS>(S, a, tx, ty, item.z); break;
+        case 9: aggregated_tile<9, MOM, TWS>(S, a, tx, ty, item.z); break;
+        case 11: aggregated_tile<11, MOM, TWS>(S, a, tx, ty, item.z); break;
+        case 13: aggregated_tile<13, MOM, TWS>(S, a, tx, ty, item.z); break;
+        default: aggregated_tile<15, MOM, TWS>(S, a, tx, ty, item.z); break;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1146,28 +1148,35 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     return check_launch("sweep epilogue");
 }
 
-int sweep_tile_width(int win) { return ((RWMAX - 2 * (win / 2)) / 8) * 8; }
+// output columns of a tile for a window and a narrowing step (Geo::TW)
+int sweep_tile_width(int win, int tws) { return ((RWMAX - 2 * (win / 2)) / 8 - tws) * 8; }
 int sweep_tile_height() { return TH; }
 
 int sweep_batch_launch(const BatchFrameDev *frames, const uint4 *items, int n_items, unsigned int *next,
                        unsigned long long *t_start, const BatchCamDev *cams, const int *hom_offsets, int n_frames,
-                       int n_hom, int moments, int ctas, void *stream)
+                       int n_hom, int moments, int ctas, int tws, void *stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
+    if (tws < 0 || tws > 1) return set_error(MVS_ERR_ARG, "tile step %d (0 or 1)", tws);
     batch_start_kernel<<<1, 1, 0, st>>>(next, t_start);
     if (n_hom > 0) homography_batch_kernel<<<ceil_div(n_hom, 128), 128, 0, st>>>(cams, hom_offsets, n_frames);
     quad_batch_kernel<<<dim3(max(1, 4 * kSMs / max(1, n_frames)), n_frames), 256, 0, st>>>(
         frames, moments == MVS_MOMENTS_COMPENSATED);
     const int sm = (int)sizeof(AggSmem);
+#define MVS_BATCH_LAUNCH(MOM, TWS)                                                                        \
+    do {                                                                                                  \
+        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MOM, TWS>,                                   \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm));               \
+        sweep_batch_kernel<MOM, TWS><<<ctas, THREADS, sm, st>>>(frames, items, n_items, next);            \
+    } while (0)
     if (moments == MVS_MOMENTS_REFERENCE) {
-        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MVS_MOMENTS_REFERENCE>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        sweep_batch_kernel<MVS_MOMENTS_REFERENCE><<<ctas, THREADS, sm, st>>>(frames, items, n_items, next);
+        if (tws == 0) MVS_BATCH_LAUNCH(MVS_MOMENTS_REFERENCE, 0);
+        else MVS_BATCH_LAUNCH(MVS_MOMENTS_REFERENCE, 1);
     } else {
-        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<MVS_MOMENTS_COMPENSATED>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        sweep_batch_kernel<MVS_MOMENTS_COMPENSATED><<<ctas, THREADS, sm, st>>>(frames, items, n_items, next);
+        if (tws == 0) MVS_BATCH_LAUNCH(MVS_MOMENTS_COMPENSATED, 0);
+        else MVS_BATCH_LAUNCH(MVS_MOMENTS_COMPENSATED, 1);
     }
+#undef MVS_BATCH_LAUNCH
     return check_launch("sweep batch");
 }
 

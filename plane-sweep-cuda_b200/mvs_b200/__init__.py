@@ -122,7 +122,8 @@ class BatchFrameDesc(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("planes_per_chunk", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32)]
+    _fields_ = [("planes_per_chunk", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32),
+                ("tile_step", C.c_int32)]
 
 
 def _sig(name, res, *args):
@@ -457,7 +458,7 @@ class Batch:
     CUDA float32 tensors, ``K1`` (3x3, 1-based), ``rel`` (list of (R, t) per
     view), ``window``, ``zfar``, optional ``std_threshold`` and the output
     tensors ``depth`` (H, W) and optional ``labels`` (int32) / ``best``.
-    ``tuning``: None (autotune) or (planes_per_chunk, ctas_per_sm, order)."""
+    ``tuning``: None (autotune) or (planes_per_chunk, ctas_per_sm, order[, tile_step])."""
 
     def __init__(self, frames, moments=MOMENTS_COMPENSATED, tuning=None):
         descs = (BatchFrameDesc * len(frames))()
@@ -497,7 +498,7 @@ class Batch:
     def tuning(self):
         t = BatchTuning()
         check(_L.mvs_batch_get_tuning(self._h, C.byref(t)))
-        return (t.planes_per_chunk, t.ctas_per_sm, t.order)
+        return (t.planes_per_chunk, t.ctas_per_sm, t.order, t.tile_step)
 
     @property
     def work_items(self):
