@@ -34,8 +34,12 @@
 //                           (kappa * Sxx) counts as flat (std 0): constant
 //                           windows, such as the zero fill outside the source,
 //                           then give NCC 0 exactly as in exact arithmetic.
+#include <cuda.h>            // CUtensorMap
+#include <cudaTypedefs.h>    // PFN_cuTensorMapEncodeTiled
 #include <math.h>
 #include <stddef.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include "common.cuh"
 
@@ -92,6 +96,7 @@ struct SweepArgs {
     unsigned long long *wta;      // AGGREGATED: [n] (cost bits << 32 | plane)
     uint16_t *cost;               // AGGREGATED: [P][n] bf16 or null
     const float4 *quad;           // AGGREGATED: [V][n] 2x2 neighbourhoods of the sources, or null
+    int *err;                     // TMA-staged form: set when a staging wait gave up
 };
 
 // ---- pass A0: warp the region into shared memory ------------------------------
@@ -350,6 +355,12 @@ __device__ __forceinline__ float4 make_quad(const float *r, int w, bool diff)
 {
     const float d00 = r[0], d01 = r[1], d10 = r[w], d11 = r[w + 1];
     if (!diff) return make_float4(d00, d01, d10, d11);
+    return make_float4(d00, d01 - d00, d10 - d00, (d11 - d10) - (d01 - d00));
+}
+
+// make_quad's difference form from four values already in registers
+__device__ __forceinline__ float4 make_quad4(float d00, float d01, float d10, float d11)
+{
     return make_float4(d00, d01 - d00, d10 - d00, (d11 - d10) - (d01 - d00));
 }
 
@@ -762,6 +773,305 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_aggregated_kernel(SweepArgs 
     aggregated_tile<WIN, MOM>(A, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// ---- aggregated mode with TMA-staged source regions ------------------------------
+//
+// The same tile, passes and arithmetic as aggregated_tile, but pass A0 reads
+// each sample's 2x2 neighbourhood from a staged copy of the source region in
+// shared memory instead of gathering it from L2.  For every (plane, view) the
+// tile region's four corners are projected (a homography maps the rectangle
+// into the hull of their images when the projective depth stays positive);
+// the bounding box, widened by one pixel for rounding and started on a
+// 16-byte column, is loaded by one cp.async.bulk.tensor (a plain TMA load of
+// this GPU's source stack, no multicast) into one of two staging buffers,
+// two (plane, view) steps ahead of its use, and an mbarrier says when it has
+// landed.  A box larger than the buffer, a corner behind the camera, or a
+// sample outside the box (rounding) falls back to the global gather for that
+// step or sample.  The staged values are the source's own bits, and the
+// difference form is formed in registers with quad_kernel's operations, so
+// the results equal aggregated_tile's bit for bit.  Each staging wait is
+// bounded (1 s of %globaltimer): on a timeout the CTA records the error,
+// waits (bounded) for its other copy in flight and leaves; the host then
+// returns MVS_ERR_TIMEOUT.
+
+constexpr int STG_W = 88, STG_H = 48;     // staged box (floats): every C2 tile region's footprint fits
+constexpr uint64_t kStageWaitNs = 1000000000ull;
+
+struct StgCtl {
+    uint64_t mbar[2];
+    int bx[2], by[2], fits[2];
+    int rx0, rx1, ry0, ry1;   // 1-based pixel range the tile region samples
+    int abort;
+};
+constexpr size_t kStgOffset = (sizeof(AggSmem) + 127) / 128 * 128;
+constexpr size_t kStgBytes = kStgOffset + 2 * sizeof(float) * STG_W * STG_H + sizeof(StgCtl) + 128;
+
+// the box of (plane, view) pair k of this chunk: bounding box of the region's
+// corners under H, or fits = 0 (thread 0)
+__device__ __forceinline__ void stage_issue(StgCtl &C, float (*box)[STG_H][STG_W], const CUtensorMap *tmap,
+                                            const float *__restrict__ H9, int view, int b)
+{
+    float H[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) H[i] = ldg(H9 + i);
+    float xmin = 3e38f, xmax = -3e38f, ymin = 3e38f, ymax = -3e38f;
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float X = (float)((c & 1) ? C.rx1 : C.rx0), Y = (float)((c & 2) ? C.ry1 : C.ry0);
+        const float q0 = H[0] * X + H[1] * Y + H[2], q1 = H[3] * X + H[4] * Y + H[5], q2 = H[6] * X + H[7] * Y + H[8];
+        ok = ok && q2 > 0.f;
+        const float xs = q0 / q2 - 1.f, ys = q1 / q2 - 1.f;
+        xmin = fminf(xmin, xs), xmax = fmaxf(xmax, xs), ymin = fminf(ymin, ys), ymax = fmaxf(ymax, ys);
+    }
+    ok = ok && xmin > -1e6f && xmax < 1e6f && ymin > -1e6f && ymax < 1e6f;   // also false for NaN
+    int bx = 0, by = 0;
+    if (ok) {
+        const int x0 = (int)floorf(xmin) - 1, x1 = (int)floorf(xmax) + 2;
+        const int y0 = (int)floorf(ymin) - 1, y1 = (int)floorf(ymax) + 2;
+        bx = x0 >= 0 ? x0 & ~3 : -((3 - x0) & ~3);   // down to a multiple of 4 columns (16 bytes)
+        by = y0;
+        ok = x1 - bx < STG_W && y1 - by < STG_H;
+    }
+    C.bx[b] = bx;
+    C.by[b] = by;
+    C.fits[b] = ok;
+    const uint32_t bar = smem_u32(&C.mbar[b]);
+    if (ok) {
+        fence_async_smem();   // the buffer's earlier generic reads before the async write
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"((uint32_t)(sizeof(float) * STG_W * STG_H))
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+            "[%5];" ::"r"(smem_u32(box[b])),
+            "l"(tmap), "r"(bx), "r"(by), "r"(view), "r"(bar)
+            : "memory");
+    } else {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+    }
+}
+
+// pass A0 from a staged box (the gather of pass_a0_rows with QUAD = false
+// semantics for the neighbourhood values, then the same interpolation)
+template <int WIN, int MOM>
+__device__ __forceinline__ void pass_a0_staged(float (*Wt)[RWMAX], const float (*box)[STG_W], int bx, int by,
+                                               const float *__restrict__ src, int w, int h, const float *Hm, float X,
+                                               const float *Yc, float shift)
+{
+    using G = Geo<WIN>;
+    constexpr int CELLS = G::A0ROWS;
+    constexpr int BATCH = 4;
+    if (threadIdx.x >= G::COLT) return;
+    const int rx = threadIdx.x % G::RW, rb = threadIdx.x / G::RW;
+    const float a0 = fmaf(Hm[0], X, Hm[2]), a1 = fmaf(Hm[3], X, Hm[5]), a2 = fmaf(Hm[6], X, Hm[8]);
+    const unsigned wm1 = __float_as_uint((float)(w - 1)), hm1 = __float_as_uint((float)(h - 1));
+#pragma unroll
+    for (int k0 = 0; k0 < CELLS; k0 += BATCH) {
+        float fa[BATCH], fb[BATCH], d00[BATCH], d01[BATCH], d10[BATCH], d11[BATCH];
+        bool ok[BATCH];
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const int k = k0 + j;
+            ok[j] = false;
+            fa[j] = fb[j] = 0.f;
+            d00[j] = d01[j] = d10[j] = d11[j] = 0.f;
+            if (k < CELLS && rb + 3 * k < G::RH) {
+                const float Y = Yc[rb + 3 * k];
+                float xs, ys;
+                if (MOM == MVS_MOMENTS_REFERENCE) {
+                    const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
+                    const float q1 = Hm[3] * X + Hm[4] * Y + Hm[5] * 1.f;
+                    const float q2 = Hm[6] * X + Hm[7] * Y + Hm[8] * 1.f;
+                    xs = q0 / q2 - 1.f;
+                    ys = q1 / q2 - 1.f;
+                } else {
+                    const float q0 = fmaf(Hm[1], Y, a0), q1 = fmaf(Hm[4], Y, a1), q2 = fmaf(Hm[7], Y, a2);
+                    float rz;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rz) : "f"(q2));
+                    xs = fmaf(q0, rz, -1.f);
+                    ys = fmaf(q1, rz, -1.f);
+                }
+                ok[j] = __float_as_uint(xs) < wm1 && __float_as_uint(ys) < hm1;
+                const float tx = __fadd_rd(xs, kFloorMagic), ty = __fadd_rd(ys, kFloorMagic);
+                fa[j] = xs - (tx - kFloorMagic);
+                fb[j] = ys - (ty - kFloorMagic);
+                if (ok[j]) {
+                    const int ix = (int)(__float_as_uint(tx) - (unsigned)kFloorMagicBits);
+                    const int iy = (int)(__float_as_uint(ty) - (unsigned)kFloorMagicBits);
+                    const unsigned lx = (unsigned)(ix - bx), ly = (unsigned)(iy - by);
+                    if (lx <= STG_W - 2u && ly <= STG_H - 2u) {
+                        d00[j] = box[ly][lx];
+                        d01[j] = box[ly][lx + 1];
+                        d10[j] = box[ly + 1][lx];
+                        d11[j] = box[ly + 1][lx + 1];
+                    } else {   // outside the staged box (rounding): the global gather
+                        const float *r0 = src + (size_t)iy * w + ix;
+                        d00[j] = ldg(r0);
+                        d01[j] = ldg(r0 + 1);
+                        d10[j] = ldg(r0 + w);
+                        d11[j] = ldg(r0 + w + 1);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const int k = k0 + j;
+            if (k >= CELLS || rb + 3 * k >= G::RH) continue;
+            const float a = fa[j], b = fb[j];
+            float v;
+            if (MOM == MVS_MOMENTS_REFERENCE) {
+                const float t1 = a * d01[j] + (1 - a) * d00[j];
+                const float t2 = a * d11[j] + (1 - a) * d10[j];
+                v = ok[j] ? b * t2 + (1 - b) * t1 : 0.f;
+            } else {
+                const float4 q = make_quad4(d00[j], d01[j], d10[j], d11[j]);
+                v = (ok[j] ? fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)) : 0.f) - shift;
+            }
+            Wt[rb + 3 * k][rx] = v;
+        }
+    }
+}
+
+// grid: (tiles_x, tiles_y, n_chunks); dynamic shared memory: kStgBytes; two CTAs per SM
+template <int WIN, int MOM>
+__global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_tma_kernel(SweepArgs a,
+                                                                          const __grid_constant__ CUtensorMap tmap)
+{
+    using G = Geo<WIN>;
+    extern __shared__ __align__(128) unsigned char stg_smem[];
+    unsigned char *base = (unsigned char *)(((uintptr_t)stg_smem + 127) & ~(uintptr_t)127);
+    AggSmem &A = *reinterpret_cast<AggSmem *>(base);
+    float (*box)[STG_H][STG_W] = reinterpret_cast<float (*)[STG_H][STG_W]>(base + kStgOffset);
+    StgCtl &C = *reinterpret_cast<StgCtl *>(base + kStgOffset + 2 * sizeof(float) * STG_W * STG_H);
+    Smem &S = A.S;
+    const int tx = blockIdx.x, ty = blockIdx.y, chunk = blockIdx.z;
+    const int x0 = tx * G::TW, y0 = ty * TH;
+    const int w = a.w, h = a.h;
+    const size_t n = (size_t)w * h;
+    const int p0 = chunk * a.planes_per_chunk, p1 = min(a.P, p0 + a.planes_per_chunk);
+    const int K = (p1 - p0) * a.V;   // (plane, view) steps of this CTA
+    if (threadIdx.x == 0) {
+        mbar_init(&C.mbar[0], 1);
+        mbar_init(&C.mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        // the clipped pixel range of the region (mirrored coordinates stay inside it)
+        C.rx0 = max(x0 - G::R, 0) + 1;
+        C.rx1 = min(x0 + G::RW - G::R - 1, w - 1) + 1;
+        C.ry0 = max(y0 - G::R, 0) + 1;
+        C.ry1 = min(y0 + G::RH - G::R - 1, h - 1) + 1;
+        C.abort = 0;
+        for (int k = 0; k < 2 && k < K; ++k) {
+            const int p = p0 + k / a.V, view = k % a.V;
+            stage_issue(C, box, &tmap, a.H + ((size_t)view * a.P + p) * 9, view, k);
+        }
+    }
+    load_ref_region<WIN, MOM>(S, a.ref, w, h, x0, y0);
+    for (int i = threadIdx.x; i < G::RH; i += THREADS) A.Yc[i] = (float)(mirror_idx(y0 - G::R + i, h) + 1);
+    __syncthreads();
+    const float shift = tile_shift<WIN, MOM>(S);
+    for (int i = threadIdx.x; i < G::RH * RWMAX; i += THREADS) {
+        const int ry = i / RWMAX, rx = i % RWMAX;
+        const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
+        A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
+    }
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
+    const int ly = b_row(), lx = b_seg() * G::RUN;
+    const int y = y0 + ly, xb = x0 + lx;
+    const bool vec_cost = G::RUN == 8 && a.cost && (w & 7) == 0 && xb + 8 <= w && ((uintptr_t)a.cost & 15) == 0;
+    uint32_t best[G::RUN];
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) best[j] = 0xffffffffu;
+    const float invV = 1.f / (float)a.V;
+    const float sh = MOM == MVS_MOMENTS_REFERENCE ? 0.f : shift;
+    if (threadIdx.x < 9 && p0 < p1) S.Hm[0][threadIdx.x] = ldg(a.H + (size_t)p0 * 9 + threadIdx.x);
+    __syncthreads();
+    int hb = 0, k = 0;
+    for (int p = p0; p < p1; ++p) {
+        float acc[G::RUN];
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) acc[j] = 0.f;
+        for (int view = 0; view < a.V; ++view, ++k) {
+            float Hm[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Hm[i] = S.Hm[hb][i];
+            const bool last_view = view + 1 == a.V;
+            const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
+            float hn = 0.f;
+            if (threadIdx.x < 9 && np < p1) hn = ldg(a.H + ((size_t)nv * a.P + np) * 9 + threadIdx.x);
+            const int b = k & 1;
+            if (!mbar_wait_bounded(&C.mbar[b], (uint32_t)((k >> 1) & 1), kStageWaitNs)) C.abort = 1;
+            if (C.fits[b])
+                pass_a0_staged<WIN, MOM>(S.Wt, box[b], C.bx[b], C.by[b], a.srcs + (size_t)view * n, w, h, Hm, Xcol,
+                                         A.Yc, sh);
+            else if (a.quad)
+                pass_a0_rows<WIN, MOM, true>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc, sh);
+            else
+                pass_a0_rows<WIN, MOM, false>(S.Wt, a.srcs + (size_t)view * n, nullptr, w, h, Hm, Xcol, A.Yc, sh);
+            if (threadIdx.x < 9) S.Hm[hb ^ 1][threadIdx.x] = hn;
+            hb ^= 1;
+            __syncthreads();   // Wt and the next homography visible; buffer b read
+            if (C.abort) {
+                if (threadIdx.x == 0) {
+                    atomicExch(a.err, 1);
+                    // the copies that may still be in flight: this step's and the next one's
+                    mbar_wait_bounded(&C.mbar[b], (uint32_t)((k >> 1) & 1), kStageWaitNs);
+                    if (k + 1 < K) mbar_wait_bounded(&C.mbar[b ^ 1], (uint32_t)(((k + 1) >> 1) & 1), kStageWaitNs);
+                }
+                return;
+            }
+            if (threadIdx.x == 0 && k + 2 < K) {
+                const int k2 = k + 2, p2 = p0 + k2 / a.V, v2 = k2 % a.V;
+                stage_issue(C, box, &tmap, a.H + ((size_t)v2 * a.P + p2) * 9, v2, b);
+            }
+            pass_a1_rows<WIN, MOM>(S.Wt, S.CS, A.Rf);
+            __syncthreads();
+            float s1[G::RUN], s2[G::RUN], s12[G::RUN];
+            row_sums<WIN, MOM>(S.CS[0], s1);
+            row_sums<WIN, MOM>(S.CS[1], s2);
+            row_sums<WIN, MOM>(S.CS[2], s12);
+            ncc_run<WIN, MOM, 0>(s1, s2, s12, A.RM[ly] + lx, A.RS[ly] + lx, a.stdthresh,
+                                 [&](int j, float c) { acc[j] += c; });
+        }
+        uint16_t cb[G::RUN];
+#pragma unroll
+        for (int j = 0; j < G::RUN; ++j) {
+            float cf = fmaf(-acc[j], invV, 1.f);
+            cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
+            cb[j] = f2bf(cf);
+            best[j] = min(best[j], ((uint32_t)cb[j] << 16) | (uint32_t)p);
+        }
+        if (a.cost && y < h) {
+            uint16_t *row = a.cost + (size_t)p * n + (size_t)y * w + xb;
+            if (vec_cost) {
+                uint4 q;
+                q.x = (uint32_t)cb[0] | ((uint32_t)cb[1 % G::RUN] << 16);
+                q.y = (uint32_t)cb[2 % G::RUN] | ((uint32_t)cb[3 % G::RUN] << 16);
+                q.z = (uint32_t)cb[4 % G::RUN] | ((uint32_t)cb[5 % G::RUN] << 16);
+                q.w = (uint32_t)cb[6 % G::RUN] | ((uint32_t)cb[7 % G::RUN] << 16);
+                *reinterpret_cast<uint4 *>(row) = q;
+            } else {
+#pragma unroll
+                for (int j = 0; j < G::RUN; ++j)
+                    if (xb + j < w) row[j] = cb[j];
+            }
+        }
+    }
+    if (y >= h) return;
+#pragma unroll
+    for (int j = 0; j < G::RUN; ++j) {
+        const int x = xb + j;
+        if (x >= w) break;
+        const bool any = best[j] != 0xffffffffu;
+        const unsigned long long key = !any ? ~0ull
+            : ((unsigned long long)__float_as_uint(bf2f((uint16_t)(best[j] >> 16))) << 32) | (best[j] & 0xffffu);
+        unsigned long long *o = a.wta + (size_t)y * w + x;
+        if (a.n_chunks == 1) *o = key;
+        else if (any) atomicMin(o, key);
+    }
+}
+
 // ---- epilogues ----------------------------------------------------------------------
 
 // sum_depthmap_NCC + element_rdivide + set_QNAN_value (kernels.cu:84-101,145-157,
@@ -1066,6 +1376,65 @@ int launch_window(int win, const SweepArgs &a, int mode, void *stream)
     return set_error(MVS_ERR_ARG, "window %d not supported (odd, 3..15)", win);
 }
 
+// The source stack [V][H][W] as a TMA tensor map (boxes of STG_W x STG_H x 1;
+// out-of-range elements read as zero).  false if the driver entry point is
+// missing or the layout does not qualify (rows must be whole 16-byte groups).
+bool make_source_map(CUtensorMap *m, const float *srcs, int w, int h, int V)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            encode = nullptr;
+        cudaGetLastError();
+    }
+    if (!encode || (w & 3) || ((uintptr_t)srcs & 15)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)V};
+    const cuuint64_t strides[2] = {(cuuint64_t)w * 4, (cuuint64_t)w * h * 4};
+    const cuuint32_t box[3] = {STG_W, STG_H, 1}, es[3] = {1, 1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)srcs, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int MOM>
+int launch_window_tma(int win, const SweepArgs &a, const CUtensorMap &tmap, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+#define MVS_SWEEP_TMA_CASE(WIN)                                                                          \
+    case WIN: {                                                                                          \
+        dim3 grid(ceil_div(a.w, Geo<WIN>::TW), ceil_div(a.h, TH), a.n_chunks);                           \
+        MVS_TRY_CUDA(cudaFuncSetAttribute(sweep_aggregated_tma_kernel<WIN, MOM>,                         \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStgBytes)); \
+        sweep_aggregated_tma_kernel<WIN, MOM><<<grid, THREADS, kStgBytes, st>>>(a, tmap);               \
+        return check_launch("sweep kernel (TMA-staged)");                                                \
+    }
+    switch (win) {
+        MVS_SWEEP_TMA_CASE(3)
+        MVS_SWEEP_TMA_CASE(5)
+        MVS_SWEEP_TMA_CASE(7)
+        MVS_SWEEP_TMA_CASE(9)
+        MVS_SWEEP_TMA_CASE(11)
+        MVS_SWEEP_TMA_CASE(13)
+        MVS_SWEEP_TMA_CASE(15)
+    }
+#undef MVS_SWEEP_TMA_CASE
+    return set_error(MVS_ERR_ARG, "window %d not supported (odd, 3..15)", win);
+}
+
+// The aggregated sweep with TMA-staged source regions is opt-in: set
+// MVS_SWEEP_STAGING=tma in the environment (looked up at every call).  It
+// needs a caller workspace (for its error word) and rows of whole 16-byte
+// groups; otherwise the gather form runs.
+bool staging_requested()
+{
+    const char *e = getenv("MVS_SWEEP_STAGING");
+    return e && strcmp(e, "tma") == 0;
+}
+
 int tiles_for(int win, int w, int h)
 {
     int tw = ((RWMAX - 2 * (win / 2)) / 8) * 8;
@@ -1119,6 +1488,16 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     a.wta = nullptr;
     a.cost = nullptr;
     a.quad = nullptr;
+    a.err = nullptr;
+    CUtensorMap tmap;
+    const bool tma = d->mode == MVS_SWEEP_AGGREGATED && quad && staging_requested() &&
+                     make_source_map(&tmap, srcs, d->width, d->height, d->n_views);
+    if (tma) {
+        // the staged form samples the sources themselves: the quad area holds its error word instead
+        a.err = reinterpret_cast<int *>(quad);
+        MVS_TRY_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), st));
+        quad = nullptr;
+    }
     if (quad) {
         const size_t total = (size_t)n * d->n_views;
         const size_t blocks = (total + 255) / 256 < (size_t)16 * kSMs ? (total + 255) / 256 : (size_t)16 * kSMs;
@@ -1135,7 +1514,12 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
         a.cost = cost;
         if (a.n_chunks > 1) MVS_TRY_CUDA(cudaMemsetAsync(scratch, 0xff, sizeof(unsigned long long) * (size_t)n, st));
     }
-    int rc = d->moments == MVS_MOMENTS_REFERENCE ? launch_window<MVS_MOMENTS_REFERENCE>(d->window, a, d->mode, stream)
+    int rc;
+    if (tma)
+        rc = d->moments == MVS_MOMENTS_REFERENCE ? launch_window_tma<MVS_MOMENTS_REFERENCE>(d->window, a, tmap, stream)
+                                                 : launch_window_tma<MVS_MOMENTS_COMPENSATED>(d->window, a, tmap, stream);
+    else
+        rc = d->moments == MVS_MOMENTS_REFERENCE ? launch_window<MVS_MOMENTS_REFERENCE>(d->window, a, d->mode, stream)
                                                  : launch_window<MVS_MOMENTS_COMPENSATED>(d->window, a, d->mode, stream);
     if (rc) return rc;
     const int eb = 256, eg = min(ceil_div(n, eb), 8 * kSMs);
@@ -1145,7 +1529,14 @@ int sweep_launch(const mvs_sweep_desc *d, const float *ref, const float *srcs, c
     } else {
         wta_finish_kernel<<<eg, eb, 0, st>>>(scratch, depths, n, d->zfar, depth, labels, best);
     }
-    return check_launch("sweep epilogue");
+    rc = check_launch("sweep epilogue");
+    if (!rc && tma) {
+        int h_err = 0;
+        MVS_TRY_CUDA(cudaMemcpyAsync(&h_err, a.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MVS_TRY_CUDA(cudaStreamSynchronize(st));
+        if (h_err) rc = set_error(MVS_ERR_TIMEOUT, "sweep: a TMA staging wait gave up");
+    }
+    return rc;
 }
 
 // output columns of a tile for a window and a narrowing step (Geo::TW)

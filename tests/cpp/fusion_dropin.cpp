@@ -6,7 +6,7 @@
 // not free it) and Resize (fusion.h:298-306: new storage, same volume).
 //
 //   fusion_dropin <in.bin> <out.bin>
-// in.bin : int32 w, h, d, n_maps, map_w, map_h; float a[3], b[3], thr, tau, lambda, sigma;
+// in.bin : int32 w, h, d, n_maps, map_w, map_h; float a[3], b[3], thr; double tau, lambda, sigma;
 //          float depth[n_maps][map_h][map_w], K[n_maps][9], R[n_maps][9], t[n_maps][3]
 // out.bin: int32 pitch, then two snapshots of the AoS rows (`pitch` bytes each,
 //          h * d rows): after the per-map iterations, and after one more U and
@@ -32,8 +32,10 @@ int main(int argc, char **argv)
     FILE *fi = std::fopen(argv[1], "rb");
     if (!fi) return fail("cannot open input");
     int32_t hdr[6];
-    float box[6], prm[4];
-    if (std::fread(hdr, 4, 6, fi) != 6 || std::fread(box, 4, 6, fi) != 6 || std::fread(prm, 4, 4, fi) != 4)
+    float box[6], thr;
+    double prm[3];   // tau, lambda, sigma: doubles, as the FusionUpdate* wrappers take them
+    if (std::fread(hdr, 4, 6, fi) != 6 || std::fread(box, 4, 6, fi) != 6 || std::fread(&thr, 4, 1, fi) != 1 ||
+        std::fread(prm, 8, 3, fi) != 3)
         return fail("short header");
     const int w = hdr[0], h = hdr[1], d = hdr[2], nm = hdr[3], mw = hdr[4], mh = hdr[5];
     std::vector<float> depth((size_t)nm * mw * mh), K((size_t)nm * 9), R((size_t)nm * 9), t((size_t)nm * 3);
@@ -53,8 +55,8 @@ int main(int argc, char **argv)
             return fail("upload");
         // fusionData is passed by value, as the reference's wrappers take it:
         // the callee's copy shares the storage and must not free it
-        FusionUpdateIteration<8>(f, d_depth, Matrix3D(&K[9 * m]), Matrix3D(&R[9 * m]), Vector3D(&t[3 * m]), prm[0],
-                                 prm[1], prm[2], prm[3], mw, mh);
+        FusionUpdateIteration<8>(f, d_depth, Matrix3D(&K[9 * m]), Matrix3D(&R[9 * m]), Vector3D(&t[3 * m]), thr,
+                                 prm[0], prm[1], prm[2], mw, mh);
     }
     const size_t pitch = (size_t)w * sizeof(fusionvoxel<8>) + 36;   // not a multiple of the voxel size
     const size_t rows = (size_t)h * d;
@@ -67,8 +69,8 @@ int main(int argc, char **argv)
         k = f;                // shallow assignment
         if (k.handle() != f.handle()) return fail("assignment does not share the volume");
     }                          // g, k go out of scope: the storage must survive
-    FusionUpdateU<8>(f, prm[1], prm[2]);
-    FusionUpdateP<8>(f, prm[3]);
+    FusionUpdateU<8>(f, prm[0], prm[1]);
+    FusionUpdateP<8>(f, prm[2]);
     if (cudaDeviceSynchronize() != cudaSuccess) return fail("CUDA error after the updates");
 
     f.copyTo(reinterpret_cast<fusionvoxel<8> *>(buf.data() + rows * pitch), pitch);

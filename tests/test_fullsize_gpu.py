@@ -60,6 +60,33 @@ def bf16_ulp(c):
 BENCH_SEED = 2   # the bench's frame (bench.py SEED + rank 0)
 
 
+def near_cutoff(H64, ps, ys, xs, win, w, h, delta=1e-3):
+    """For entries (plane ps[i], pixel (ys[i], xs[i])): whether a sample of the
+    pixel's window (rows and columns mirrored at the frame border, as the box
+    means read them) warped by some view's FP64 homography lies within `delta`
+    pixels of the out-of-image cut-off of bilinear_interpolation
+    (kernels.cu:4-29: the sample is 0 unless 0 <= x < W-1 and 0 <= y < H-1).
+    There a sample in FP32 and in FP64 can fall on opposite sides."""
+    r = win // 2
+    off = np.arange(-r, r + 1)
+
+    def mirror(k, n):
+        k = np.abs(k)
+        return np.where(k > n - 1, 2 * (n - 1) - k, k)
+    out = np.zeros(len(ps), bool)
+    for i, (p, y, x) in enumerate(zip(ps, ys, xs)):
+        yy, xx = np.meshgrid(mirror(y + off, h), mirror(x + off, w), indexing="ij")
+        pts = np.stack([xx + 1.0, yy + 1.0, np.ones_like(xx, float)]).reshape(3, -1)
+        for v in range(H64.shape[0]):
+            q = H64[v, p].reshape(3, 3) @ pts
+            X, Y = q[0] / q[2] - 1, q[1] / q[2] - 1
+            d = np.min(np.minimum.reduce([np.abs(X), np.abs(X - (w - 1)), np.abs(Y), np.abs(Y - (h - 1))]))
+            if d < delta:
+                out[i] = True
+                break
+    return out
+
+
 @pytest.fixture(scope="module")
 def c2_frame():
     return scenes.config_full(seed=BENCH_SEED)
@@ -77,9 +104,12 @@ def c2_sweep(cuda, c2_frame):
 def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
     """Labels identical to the FP64 oracle's on >= 99.9% of the pixels; every
     other pixel within one plane, or a tie that BF16 storage cannot separate
-    (the FP64 costs of the two planes within one BF16 step).  The stored BF16
-    costs equal the FP64 cost rounded to BF16 except where the FP64 cost lies
-    within rounding distance of a BF16 boundary (at most one BF16 step off)."""
+    (the FP64 costs of the two planes within one BF16 step), or a pixel whose
+    window reaches the reference's out-of-image cut-off of the warp.  Every
+    stored cost is within 1e-4 of the FP64 cost beyond its BF16 rounding,
+    except entries at that cut-off (a sample within 1e-3 px of it, where FP32
+    and FP64 coordinates fall on opposite sides and the view's NCC changes
+    wholesale); their count is recorded."""
     fr, planes, win = c2_frame
     poses = [(c.R, c.t) for c in fr.src_cams]
     V = len(poses)
@@ -91,6 +121,8 @@ def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
     excess = []   # per band: |GPU BF16 cost - FP64 cost| beyond half a BF16 step of the FP64 cost
     win_err = []
     odd = []      # pixels more than one plane off that are not BF16 ties
+    n_big_cut, big_other = 0, []   # cost entries off by more than 1e-4: at the warp cut-off / elsewhere
+    n_odd_cut = 0   # pixels more than one plane off, not ties, at the warp cut-off
     for y0 in range(0, h, 96):
         y1 = min(h, y0 + 96)
         c64 = np.maximum(1.0 - po.sweep_ncc_band(fr.ref, fr.srcs, H64, win, y0, y1) / V, 0.0)
@@ -99,7 +131,14 @@ def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
         g = gl[y0:y1]
         gc = (gbits[:, y0:y1].astype(np.uint32) << 16).view(np.float32)
         n_cost_same += int(np.sum(gc == cb))
-        excess.append(np.maximum(np.abs(gc - c64) - 0.5 * bf16_ulp(np.maximum(c64, 2.0 ** -30)), 0.0).ravel())
+        ex = np.maximum(np.abs(gc - c64) - 0.5 * bf16_ulp(np.maximum(c64, 2.0 ** -30)), 0.0)
+        big = np.nonzero(ex > 1e-4)   # (plane, row, column) entries with a real FP32 error
+        if big[0].size:
+            cut = near_cutoff(H64, big[0], big[1] + y0, big[2], win, w, h)
+            n_big_cut += int(cut.sum())
+            big_other += [(int(p_), int(y_ + y0), int(x_), float(ex[p_, y_, x_]))
+                          for p_, y_, x_, c in zip(*big, cut) if not c]
+        excess.append(np.where(ex > 1e-4, 0.0, ex).ravel())
         d = np.abs(g.astype(np.int64) - ol)
         n_same += int(np.sum(d == 0))
         n_near += int(np.sum(d <= 1))
@@ -108,7 +147,11 @@ def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
         cg, co = c64[g[far], yy, xx], c64[ol[far], yy, xx]
         tie = np.abs(cg - co) <= bf16_ulp(np.maximum(co, 2.0 ** -20))
         n_tie += int(np.sum(tie))
-        for y, x in zip(yy[~tie], xx[~tie]):
+        cut = near_cutoff(H64, np.concatenate([g[far][~tie], ol[far][~tie]]),
+                          np.concatenate([yy[~tie], yy[~tie]]) + y0, np.concatenate([xx[~tie], xx[~tie]]), win, w, h)
+        cut = cut[:int((~tie).sum())] | cut[int((~tie).sum()):]
+        n_odd_cut += int(cut.sum())
+        for y, x in zip(yy[~tie][~cut], xx[~tie][~cut]):
             odd.append({"y": int(y + y0), "x": int(x), "label_gpu": int(g[y, x]), "label_fp64": int(ol[y, x]),
                         "fp64_cost_at_gpu_label": float(c64[g[y, x], y, x]),
                         "fp64_cost_at_fp64_label": float(c64[ol[y, x], y, x]),
@@ -121,16 +164,17 @@ def test_c2_sweep_full_frame_vs_fp64_oracle(c2_frame, c2_sweep):
     win_err = np.concatenate(win_err)
     excess = np.concatenate(excess)
     rep = {"pixels": npx, "labels_identical": n_same / npx, "labels_within_one_plane": n_near / npx,
-           "labels_beyond_one_plane_bf16_ties": n_tie / npx, "labels_beyond_one_plane_not_ties": odd[:16],
+           "labels_beyond_one_plane_bf16_ties": n_tie / npx, "labels_beyond_one_plane_at_warp_cutoff": n_odd_cut,
+           "labels_beyond_one_plane_other": odd[:16],
            "cost_entries_identical_bf16": n_cost_same / (npx * len(planes)),
            "cost_abs_err_beyond_bf16_rounding": {"p99.9": q(excess, 0.999), "p99.99": q(excess, 0.9999),
-                                                 "max": float(excess.max())},
+                                                 "max_off_cutoff": float(excess.max())},
+           "cost_entries_above_1e-4_at_warp_cutoff": n_big_cut, "cost_entries_above_1e-4_other": big_other[:16],
            "winning_cost_abs_err_vs_fp64_incl_bf16_rounding": {"p50": q(win_err, 0.5), "p99.9": q(win_err, 0.999),
                                                                "max": float(win_err.max())}}
     REPORT["c2_sweep_aggregated_bf16_wta"] = rep
     assert rep["labels_identical"] >= 0.999, rep
-    assert not odd, rep
-    assert rep["cost_abs_err_beyond_bf16_rounding"]["p99.99"] <= 1e-4, rep
+    assert not odd and not big_other, rep
 
 
 def test_c3_fusion_vs_oracle(cuda):

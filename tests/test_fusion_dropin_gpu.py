@@ -59,7 +59,8 @@ def test_cpp_fusion_dropin_matches_reference_and_c_abi(cuda, golden, tmp_path):
     with open(inp, "wb") as f:
         np.asarray([w, h, d, nm, mw, mh], np.int32).tofile(f)
         np.concatenate([g["vol_min"], g["vol_max"]]).astype(np.float32).tofile(f)
-        np.asarray([thr, tau, lam, sigma], np.float32).tofile(f)
+        np.asarray([thr], np.float32).tofile(f)
+        np.asarray([tau, lam, sigma], np.float64).tofile(f)
         for k in ("depths", "K", "R", "t"):
             np.ascontiguousarray(g[k], np.float32).tofile(f)
     exe = _build(tmp_path)

@@ -277,3 +277,29 @@ def test_full_size_properties(cuda):
     np.testing.assert_allclose(r1["depth"], want, rtol=1e-6)
     rel = np.abs(r1["depth"] - fr.depth_gt) / fr.depth_gt
     assert np.median(rel[cnt > 0]) < 0.03
+
+
+@pytest.mark.parametrize("moments,win", [(M.MOMENTS_COMPENSATED, 9), (M.MOMENTS_COMPENSATED, 15),
+                                         (M.MOMENTS_REFERENCE, 5)])
+def test_tma_staged_form_equals_gather_form(cuda, moments, win, monkeypatch):
+    """The aggregated sweep with TMA-staged source regions (MVS_SWEEP_STAGING=tma)
+    against the gather form: cost volume, labels, depth and best cost bit for
+    bit, at 640x480 with 8 views and 96 planes, and on a frame whose rows are
+    not whole 16-byte groups (the gather form then runs)."""
+    fr, planes, _ = scenes.config_full(seed=2)
+    planes = planes[::4].copy() if win == 9 else planes[::8].copy()
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    args = dict(K=fr.ref_cam.K_1based, Rref=fr.ref_cam.R, tref=fr.ref_cam.t, poses=poses, moments=moments,
+                mode=M.SWEEP_AGGREGATED, zfar=8.0, cost=True)
+    monkeypatch.delenv("MVS_SWEEP_STAGING", raising=False)
+    want = run_sweep(cuda, fr.ref, fr.srcs, planes, win, **args)
+    monkeypatch.setenv("MVS_SWEEP_STAGING", "tma")
+    got = run_sweep(cuda, fr.ref, fr.srcs, planes, win, **args)
+    for k in ("cost", "label", "depth", "best"):
+        np.testing.assert_array_equal(got[k], want[k])
+    # 638 columns: rows of 2552 bytes, not whole 16-byte groups
+    ref, srcs = fr.ref[:, :638].copy(), [s[:, :638].copy() for s in fr.srcs]
+    got = run_sweep(cuda, ref, srcs, planes[:16], win, **args)
+    monkeypatch.delenv("MVS_SWEEP_STAGING")
+    want = run_sweep(cuda, ref, srcs, planes[:16], win, **args)
+    np.testing.assert_array_equal(got["label"], want["label"])
