@@ -418,12 +418,14 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
         if (tid == 0) {
             tc_fence_after();
             const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
+            // K-step major: consecutive MMAs go to the 9 taps' different
+            // accumulators, so they do not wait on one another
 #pragma unroll 1
-            for (int t = 0; t < 9; ++t) {
-                const int ky = t / 3, kx = t - 3 * ky;
+            for (int ks = 0; ks < 8; ++ks) {
+                const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
 #pragma unroll
-                for (int ks = 0; ks < 8; ++ks) {
-                    const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
+                for (int t = 0; t < 9; ++t) {
+                    const int ky = t / 3, kx = t - 3 * ky;
                     const uint64_t bd = smem_desc(bb + ((2 * ks + ky) * HW_ + kx) * 16, HW_ * 16, HALO_PIX * 16);
                     mma_bf16(tmem + t * NC, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
                 }

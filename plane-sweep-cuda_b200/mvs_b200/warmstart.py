@@ -308,6 +308,48 @@ def evaluate(seeds, cfg: FrameConfig, params, norm, prm=None, dual_sigma=WARM_DU
     return rows
 
 
+def layer_timing(B, reps, shapes, height=480, width=640):
+    """Per-layer device times (ms, CUDA events, mean of `reps` after one
+    warm-up) of the tensor-core 3x3 convolution: forward (bias + ReLU), weight
+    gradient alone (conv3x3_backward without dx) and weight + input gradient.
+    Launch order per shape: forward x (1 + reps), then backward x (1 + reps)
+    without dx, then with dx."""
+    import torch
+    import mvs_b200 as M
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev).manual_seed(0)
+    rows = []
+    for cin, cout, lvl in shapes:
+        H, W = height >> lvl, width >> lvl
+        x = (torch.rand((B, H, W, cin), device=dev, generator=g) - 0.3).to(torch.bfloat16).view(torch.int16)
+        dz = (torch.rand((B, H, W, cout), device=dev, generator=g) - 0.5).to(torch.bfloat16).view(torch.int16)
+        w = torch.rand((cout, cin, 3, 3), device=dev, generator=g) * 0.1
+        bias = torch.zeros(cout, device=dev)
+        out = torch.empty((B, H, W, cout), dtype=torch.int16, device=dev)
+        dx = torch.empty_like(x)
+        dw = torch.zeros((cout, cin, 3, 3), device=dev)
+        wpack = torch.empty(2 * 9 * cin * cout, dtype=torch.int16, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        res = {}
+        for name, fn in (("forward", lambda: M.conv3x3_forward(x, w, bias, True, out, wpack, err)),
+                         ("wgrad", lambda: M.conv3x3_backward(x, w, dz, False, None, dw, None, wpack, err)),
+                         ("wgrad_dgrad", lambda: M.conv3x3_backward(x, w, dz, True, dx, dw, None, wpack, err))):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            res[name + "_ms"] = e0.elapsed_time(e1) / reps
+        assert int(err.item()) == 0, "a tensor-core wait gave up"
+        flops = 2.0 * B * H * W * 9 * cin * cout
+        rows.append(dict(cin=cin, cout=cout, level=lvl, batch=B, height=H, width=W, gflop=flops / 1e9,
+                         input_mb=x.numel() * 2 / 1e6, **res))
+        print(rows[-1], flush=True)
+    return rows
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -323,7 +365,16 @@ def main(argv=None):
     tm = sub.add_parser("timing", help="device time of the network's forward pass and training step")
     tm.add_argument("--batch", type=int, default=4)
     tm.add_argument("--reps", type=int, default=10)
+    ly = sub.add_parser("layers", help="device time of single 3x3 layers: forward, weight and input gradient")
+    ly.add_argument("--batch", type=int, default=4)
+    ly.add_argument("--reps", type=int, default=5)
+    ly.add_argument("--shapes", default="16x16@0,48x16@0,32x32@1,128x128@3",
+                    help="cin x cout @ pyramid level, comma separated (level l: H/2^l x W/2^l)")
     a = ap.parse_args(argv)
+    if a.cmd == "layers":
+        layer_timing(a.batch, a.reps, [(int(c.split("@")[0].split("x")[0]), int(c.split("@")[0].split("x")[1]),
+                                        int(c.split("@")[1])) for c in a.shapes.split(",")])
+        return
     import mvs_b200 as M
     cfg = FrameConfig()
     if a.cmd == "timing":
