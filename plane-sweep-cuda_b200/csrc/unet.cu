@@ -318,15 +318,20 @@ int launch_conv(const bf16 *in, int cin, const bf16 *wpack, const float *bias, c
 }
 
 // ---------------------------------------------------------------------------
-// weight gradient on tensor cores: for every tap t,
-//   D_t[co][ci] += sum_p dz[p][co] * x[p + off_t][ci]
-// with K = pixels.  A = dz^T (M = co, padded to 128 rows of zeros) and
-// B = x_t^T (N = a chunk of NC input channels) are both MN-major: in shared
-// memory dz sits as [co/8][pixel][8] and x as the same halo tile as the
-// forward pass, [ci/8][halo pixel][8], so one K step of 16 pixels (two tile
-// rows) of tap t is the halo addressed from tap t's offset.  Each CTA sums a
-// run of pixel tiles into 9 accumulators (9 x NC TMEM columns) and adds them
-// to the FP32 gradient with one atomic per weight.
+// weight gradient on tensor cores: for every tap t = (ky, kx),
+//   D[co][t][ci] += sum_p dz[p][co] * x[p + off_t][ci]
+// with K = pixels, for one chunk of 16 input channels per CTA.  A = dz^T
+// (M = co, padded to 128 rows of zeros) and B = the nine tap-shifted copies of
+// the input tile (N = 9 taps x 16 channels = 144) are both MN-major with the
+// same layout, [8-group][pixel][8]: A as [co/8][pixel][8], B as
+// [tap][ci/8][pixel][8] where plane (t, g) holds x at the tile's pixels shifted
+// by tap t's offset.  One K step of 16 pixels (two tile rows) is then a single
+// MMA for all nine taps (8 per tile, with N = 144), instead of one MMA per tap
+// (72 with N = 16).  Tiles stream through a three-stage cp.async pipeline (each
+// stage's copies are one commit group); an mbarrier signalled by
+// tcgen05.commit says when a stage's MMAs are done and it may be refilled.
+// Each CTA sums a run of pixel tiles in TMEM (144 columns) and adds them to
+// the FP32 gradient with one atomic per weight.
 // ---------------------------------------------------------------------------
 
 struct WgArgs {
@@ -338,43 +343,45 @@ struct WgArgs {
 };
 
 constexpr int WG_TC_THREADS = 128;
+constexpr int WG_NC = 16;                           // input channels per CTA
+constexpr int WG_PLANES = 9 * WG_NC / 8;            // 18 B planes: (tap, channel group)
+constexpr int WG_STAGES = 3;
 
-template <int NC>
 struct WgSmem {
-    static constexpr int A_BYTES = 16 * 128 * 16;            // 16 co8 groups x 128 pixels x 16 B
-    static constexpr int B_BYTES = (NC / 8) * HALO_PIX * 16;
+    static constexpr int A_BYTES = 16 * 128 * 16;          // 16 co8 groups x 128 pixels x 16 B
+    static constexpr int B_BYTES = WG_PLANES * 128 * 16;   // 18 planes x 128 pixels x 16 B
     static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int USED = 2 * STAGE + 64;
-    // at least 116 KB so that one CTA holds an SM (its 512 TMEM columns)
-    static constexpr int BYTES = USED > 116 * 1024 ? USED : 116 * 1024;
+    static constexpr int BYTES = WG_STAGES * STAGE + 64;
 };
 
 // MN-major descriptors have the instruction descriptor's transpose bits set
 __host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) { return idesc_bf16(M, N) | (1u << 15) | (1u << 16); }
 
-template <int NC>
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 {
-    using S = WgSmem<NC>;
+    using S = WgSmem;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = (uint64_t *)(smem + 2 * S::STAGE);
-    uint32_t *tmem_slot = (uint32_t *)(smem + 2 * S::STAGE + 16);
+    uint64_t *bars = (uint64_t *)(smem + WG_STAGES * S::STAGE);
+    uint32_t *tmem_slot = (uint32_t *)(smem + WG_STAGES * S::STAGE + 32);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ci0 = blockIdx.y * NC, co0 = blockIdx.z * 128;
+    const int ci0 = blockIdx.y * WG_NC, co0 = blockIdx.z * 128;
     const int t_begin = blockIdx.x * a.tiles_per_cta;
     const int t_end = min(t_begin + a.tiles_per_cta, a.n_tiles);
     const int H = a.H, W = a.W, cin = a.cin, cout = a.cout;
     const size_t img = (size_t)H * W;
-    constexpr int TMEM_COLS = 9 * NC <= 256 ? 256 : 512;
+    constexpr int TMEM_COLS = 256;   // 144 used
 
     if (warp == 0) tmem_alloc(tmem_slot, TMEM_COLS);
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int k = 0; k < WG_STAGES; ++k) mbar_init(&bars[k], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // rows co >= cout of A stay zero in both stages
-    for (int k = tid; k < 2 * S::STAGE / 16; k += WG_TC_THREADS) ((uint4 *)smem)[k] = make_uint4(0, 0, 0, 0);
+    // rows co >= cout of A stay zero in every stage
+    for (int k = tid; k < WG_STAGES * S::STAGE / 16; k += WG_TC_THREADS) ((uint4 *)smem)[k] = make_uint4(0, 0, 0, 0);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -382,6 +389,7 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
     const uint32_t tmem = *tmem_slot;
     const uint32_t sbase = smem_u32(smem);
 
+    // cp.async of one tile into stage s (one commit group)
     auto load = [&](int tile, int s) {
         const int b = tile / (a.tiles_x * a.tiles_y), r = tile - b * a.tiles_x * a.tiles_y;
         const int y0 = (r / a.tiles_x) * TH, x0 = (r % a.tiles_x) * TW;
@@ -394,61 +402,60 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
             const bf16 *src = a.dz + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cout + co0 + 8 * g;
             cp_async16(ab + (g * 128 + m) * 16, src, ok);
         }
-        for (int k = tid; k < (NC / 8) * HALO_PIX; k += WG_TC_THREADS) {
-            const int g = k / HALO_PIX, pix = k - g * HALO_PIX;
-            const int hy = pix / HW_, hx = pix - hy * HW_;
-            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
+        for (int k = tid; k < WG_PLANES * 128; k += WG_TC_THREADS) {
+            const int pl = k >> 7, m = k & 127;          // plane (tap t, channel group g), pixel m
+            const int t = pl >> 1, g = pl & 1, ky = t / 3, kx = t - 3 * ky;
+            const int gy = y0 + (m >> 3) + ky - 1, gx = x0 + (m & 7) + kx - 1;
             const bool ok = gy >= 0 && gy < H && gx >= 0 && gx < W;
             const bf16 *src = a.x + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + ci0 + 8 * g;
-            cp_async16(bb + (g * HALO_PIX + pix) * 16, src, ok);
+            cp_async16(bb + (pl * 128 + m) * 16, src, ok);
         }
-        cp_async_wait_all();
-        fence_async_smem();
+        cp_async_commit();
     };
 
-    constexpr uint32_t idesc = idesc_bf16_mn(128, NC);
+    constexpr uint32_t idesc = idesc_bf16_mn(128, 9 * WG_NC);
     const int n = t_end - t_begin;
     bool failed = false;
-    if (n > 0) {
-        load(t_begin, 0);
-        __syncthreads();
-    }
+    int last = -1;   // the last tile whose MMAs were issued (the same in every thread)
+    for (int k = 0; k < WG_STAGES - 1 && k < n; ++k) load(t_begin + k, k);
     for (int c = 0; c < n; ++c) {
-        const int s = c & 1;
+        const int s = c % WG_STAGES;
+        if (c + 1 < n) cp_async_wait_group<1>();   // tile c landed (tile c + 1 may be in flight)
+        else cp_async_wait_group<0>();
+        fence_async_smem();
+        __syncthreads();
         if (tid == 0) {
             tc_fence_after();
             const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
-            // K-step major: consecutive MMAs go to the 9 taps' different
-            // accumulators, so they do not wait on one another
-#pragma unroll 1
+#pragma unroll
             for (int ks = 0; ks < 8; ++ks) {
                 const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
-#pragma unroll
-                for (int t = 0; t < 9; ++t) {
-                    const int ky = t / 3, kx = t - 3 * ky;
-                    const uint64_t bd = smem_desc(bb + ((2 * ks + ky) * HW_ + kx) * 16, HW_ * 16, HALO_PIX * 16);
-                    mma_bf16(tmem + t * NC, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-                }
+                const uint64_t bd = smem_desc(bb + ks * 256, 128, 128 * 16);
+                mma_bf16(tmem, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
             }
             mma_commit(&bars[s]);
         }
-        if (c + 1 < n) {
+        last = c;
+        // refill the stage that tile c - 1's MMAs read once they are done
+        if (c + WG_STAGES - 1 < n) {
+            const int sr = (c + WG_STAGES - 1) % WG_STAGES;
             if (c >= 1) {
-                const bool ok = mbar_wait_bounded(&bars[s ^ 1], ((c - 1) >> 1) & 1, kWaitNs);
+                const bool ok = mbar_wait_bounded(&bars[sr], (uint32_t)(((c - 1) / WG_STAGES) & 1), kWaitNs);
                 failed = __syncthreads_or(!ok) != 0;
                 if (failed) break;
             }
-            load(t_begin + c + 1, s ^ 1);
-            __syncthreads();
+            load(t_begin + c + WG_STAGES - 1, sr);
         }
     }
-    if (!failed && n > 0) {
-        const bool ok = mbar_wait_bounded(&bars[(n - 1) & 1], ((n - 1) >> 1) & 1, kWaitNs);
+    if (!failed && last >= 0) {
+        const bool ok = mbar_wait_bounded(&bars[last % WG_STAGES], (uint32_t)((last / WG_STAGES) & 1), kWaitNs);
         failed = __syncthreads_or(!ok) != 0;
     }
     if (failed) {
         if (tid == 0) atomicExch(a.err, 1);
-        mbar_wait_bounded(&bars[(n - 1) & 1], ((n - 1) >> 1) & 1, kWaitNs);
+        cp_async_wait_group<0>();   // copies in flight
+        if (last >= 0)              // the MMAs in flight (they complete in order)
+            mbar_wait_bounded(&bars[last % WG_STAGES], (uint32_t)((last / WG_STAGES) & 1), kWaitNs);
         tc_fence_before();
         __syncthreads();
         if (warp == 0) {
@@ -459,18 +466,16 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
     }
     tc_fence_after();
     if (n > 0) {
+        // D[co][n], n = tap * 16 + channel: TMEM lane = co (warp w holds lanes 32w..32w+31)
         const int co = co0 + warp * 32 + lane;
 #pragma unroll 1
         for (int t = 0; t < 9; ++t) {
-#pragma unroll 1
-            for (int c0 = 0; c0 < NC; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + t * NC + c0, v);
-                if (co < cout) {
-                    float *dst = a.dW + ((size_t)co * cin + ci0 + c0) * 9 + t;
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + t * WG_NC, v);
+            if (co < cout) {
+                float *dst = a.dW + ((size_t)co * cin + ci0) * 9 + t;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) atomicAdd(dst + 9 * j, v[j]);
-                }
+                for (int j = 0; j < 16; ++j) atomicAdd(dst + 9 * j, v[j]);
             }
         }
     }
@@ -482,31 +487,19 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
     }
 }
 
-template <int NC>
-int launch_wgrad_tc_t(WgArgs a, int n_chunks, cudaStream_t st)
-{
-    using S = WgSmem<NC>;
-    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
-    const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
-    wgrad_tc_kernel<NC><<<dim3(ctas, n_chunks, ceil_div(a.cout, 128)), WG_TC_THREADS, S::BYTES, st>>>(a);
-    return MVS_OK;
-}
-
 int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, int *err,
                     cudaStream_t st)
 {
-    if (cout % 8 || cin % 16) return set_error(MVS_ERR_ARG, "wgrad: cin %d, cout %d", cin, cout);
-    const int nc = cin % 48 == 0 ? 48 : cin % 32 == 0 ? 32 : 16;
+    if (cout % 8 || cin % WG_NC) return set_error(MVS_ERR_ARG, "wgrad: cin %d, cout %d", cin, cout);
     WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0};
     a.n_tiles = B * a.tiles_x * a.tiles_y;
-    const int chunks = cin / nc;
-    // about two waves of CTAs over the SMs
-    a.tiles_per_cta = std::max(1, a.n_tiles * chunks / (2 * kSMs));
-    switch (nc) {
-    case 16: return launch_wgrad_tc_t<16>(a, chunks, st);
-    case 32: return launch_wgrad_tc_t<32>(a, chunks, st);
-    default: return launch_wgrad_tc_t<48>(a, chunks, st);
-    }
+    const int chunks = cin / WG_NC, coblocks = ceil_div(cout, 128);
+    // about two waves of CTAs over the SMs (one CTA per SM: three stages fill its shared memory)
+    a.tiles_per_cta = std::max(1, a.n_tiles * chunks * coblocks / (2 * kSMs));
+    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WgSmem::BYTES));
+    const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
+    wgrad_tc_kernel<<<dim3(ctas, chunks, coblocks), WG_TC_THREADS, WgSmem::BYTES, st>>>(a);
+    return MVS_OK;
 }
 
 // ---------------------------------------------------------------------------
