@@ -494,8 +494,11 @@ int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int
     WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0};
     a.n_tiles = B * a.tiles_x * a.tiles_y;
     const int chunks = cin / WG_NC, coblocks = ceil_div(cout, 128);
-    // about two waves of CTAs over the SMs (one CTA per SM: three stages fill its shared memory)
-    a.tiles_per_cta = std::max(1, a.n_tiles * chunks * coblocks / (2 * kSMs));
+    // one wave: three stages fill an SM's shared memory, so one CTA per SM; the
+    // CTAs of every (chunk, output block) split the tiles evenly, at most kSMs
+    // CTAs in all (a last wave of a few CTAs would cost a whole run of tiles)
+    const int xctas = std::max(1, kSMs / (chunks * coblocks));
+    a.tiles_per_cta = ceil_div(a.n_tiles, xctas);
     MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WgSmem::BYTES));
     const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
     wgrad_tc_kernel<<<dim3(ctas, chunks, coblocks), WG_TC_THREADS, WgSmem::BYTES, st>>>(a);
