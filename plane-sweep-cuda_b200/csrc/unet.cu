@@ -320,18 +320,20 @@ int launch_conv(const bf16 *in, int cin, const bf16 *wpack, const float *bias, c
 // ---------------------------------------------------------------------------
 // weight gradient on tensor cores: for every tap t = (ky, kx),
 //   D[co][t][ci] += sum_p dz[p][co] * x[p + off_t][ci]
-// with K = pixels, for one chunk of 16 input channels per CTA.  A = dz^T
-// (M = co, padded to 128 rows of zeros) and B = the nine tap-shifted copies of
-// the input tile (N = 9 taps x 16 channels = 144) are both MN-major with the
-// same layout, [8-group][pixel][8]: A as [co/8][pixel][8], B as
-// [tap][ci/8][pixel][8] where plane (t, g) holds x at the tile's pixels shifted
-// by tap t's offset.  One K step of 16 pixels (two tile rows) is then a single
-// MMA for all nine taps (8 per tile, with N = 144), instead of one MMA per tap
-// (72 with N = 16).  Tiles stream through a three-stage cp.async pipeline (each
-// stage's copies are one commit group); an mbarrier signalled by
-// tcgen05.commit says when a stage's MMAs are done and it may be refilled.
-// Each CTA sums a run of pixel tiles in TMEM (144 columns) and adds them to
-// the FP32 gradient with one atomic per weight.
+// with K = pixels, for 16-channel chunks of the input.  A = dz^T (M = co,
+// padded to 128 rows of zeros) and B = the nine tap-shifted copies of the
+// input tile (N = 9 taps x 16 channels = 144) are both MN-major with the same
+// layout, [8-group][pixel][8]: A as [co/8][pixel][8], B as
+// [tap][ci/8][pixel][8] where plane (t, g) holds x at the tile's pixels
+// shifted by tap t's offset.  One K step of 16 pixels (two tile rows) is then
+// a single MMA for all nine taps (8 per tile, with N = 144), instead of one
+// MMA per tap (72 with N = 16).  A CTA takes NCH = 1 or 2 chunks (16 or 32
+// input channels) against one staged dz tile: NCH MMAs per K step into NCH
+// accumulators.  Tiles stream through a cp.async pipeline of three stages
+// (NCH = 1) or two (NCH = 2), each stage's copies one commit group; an
+// mbarrier signalled by tcgen05.commit says when a stage's MMAs are done and
+// it may be refilled.  Each CTA sums a run of pixel tiles in TMEM (144 NCH
+// columns) and adds them to the FP32 gradient with one atomic per weight.
 // ---------------------------------------------------------------------------
 
 struct WgArgs {
@@ -340,18 +342,20 @@ struct WgArgs {
     float *dW;        // [cout][cin][9]
     int *err;
     int B, H, W, cin, cout, tiles_x, tiles_y, tiles_per_cta, n_tiles;
+    int ci_base;      // first input channel of blockIdx.y == 0
 };
 
 constexpr int WG_TC_THREADS = 128;
-constexpr int WG_NC = 16;                           // input channels per CTA
-constexpr int WG_PLANES = 9 * WG_NC / 8;            // 18 B planes: (tap, channel group)
-constexpr int WG_STAGES = 3;
+constexpr int WG_NC = 16;                           // input channels per chunk
+constexpr int WG_PLANES = 9 * WG_NC / 8;            // 18 B planes per chunk: (tap, channel group)
 
+template <int NCH>
 struct WgSmem {
-    static constexpr int A_BYTES = 16 * 128 * 16;          // 16 co8 groups x 128 pixels x 16 B
-    static constexpr int B_BYTES = WG_PLANES * 128 * 16;   // 18 planes x 128 pixels x 16 B
-    static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int BYTES = WG_STAGES * STAGE + 64;
+    static constexpr int STAGES = NCH == 1 ? 3 : 2;
+    static constexpr int A_BYTES = 16 * 128 * 16;                // 16 co8 groups x 128 pixels x 16 B
+    static constexpr int CHUNK_BYTES = WG_PLANES * 128 * 16;     // 18 planes x 128 pixels x 16 B
+    static constexpr int STAGE = A_BYTES + NCH * CHUNK_BYTES;
+    static constexpr int BYTES = STAGES * STAGE + 64;
 };
 
 // MN-major descriptors have the instruction descriptor's transpose bits set
@@ -361,19 +365,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+template <int NCH>
 __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 {
-    using S = WgSmem;
+    using S = WgSmem<NCH>;
+    constexpr int WG_STAGES = S::STAGES;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = (uint64_t *)(smem + WG_STAGES * S::STAGE);
     uint32_t *tmem_slot = (uint32_t *)(smem + WG_STAGES * S::STAGE + 32);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ci0 = blockIdx.y * WG_NC, co0 = blockIdx.z * 128;
+    const int ci0 = a.ci_base + blockIdx.y * NCH * WG_NC, co0 = blockIdx.z * 128;
     const int t_begin = blockIdx.x * a.tiles_per_cta;
     const int t_end = min(t_begin + a.tiles_per_cta, a.n_tiles);
     const int H = a.H, W = a.W, cin = a.cin, cout = a.cout;
     const size_t img = (size_t)H * W;
-    constexpr int TMEM_COLS = 256;   // 144 used
+    constexpr int TMEM_COLS = NCH == 1 ? 256 : 512;   // 144 NCH used
 
     if (warp == 0) tmem_alloc(tmem_slot, TMEM_COLS);
     if (tid == 0) {
@@ -402,12 +408,14 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
             const bf16 *src = a.dz + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cout + co0 + 8 * g;
             cp_async16(ab + (g * 128 + m) * 16, src, ok);
         }
-        for (int k = tid; k < WG_PLANES * 128; k += WG_TC_THREADS) {
-            const int pl = k >> 7, m = k & 127;          // plane (tap t, channel group g), pixel m
-            const int t = pl >> 1, g = pl & 1, ky = t / 3, kx = t - 3 * ky;
+        for (int k = tid; k < NCH * WG_PLANES * 128; k += WG_TC_THREADS) {
+            const int pl = k >> 7, m = k & 127;          // plane (chunk j, tap t, channel group g), pixel m
+            const int j = pl / WG_PLANES, q = pl - j * WG_PLANES;
+            const int t = q >> 1, g = q & 1, ky = t / 3, kx = t - 3 * ky;
             const int gy = y0 + (m >> 3) + ky - 1, gx = x0 + (m & 7) + kx - 1;
             const bool ok = gy >= 0 && gy < H && gx >= 0 && gx < W;
-            const bf16 *src = a.x + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + ci0 + 8 * g;
+            const bf16 *src =
+                a.x + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + ci0 + WG_NC * j + 8 * g;
             cp_async16(bb + (pl * 128 + m) * 16, src, ok);
         }
         cp_async_commit();
@@ -420,7 +428,7 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
     for (int k = 0; k < WG_STAGES - 1 && k < n; ++k) load(t_begin + k, k);
     for (int c = 0; c < n; ++c) {
         const int s = c % WG_STAGES;
-        if (c + 1 < n) cp_async_wait_group<1>();   // tile c landed (tile c + 1 may be in flight)
+        if (WG_STAGES == 3 && c + 1 < n) cp_async_wait_group<1>();   // tile c landed (c + 1 may be in flight)
         else cp_async_wait_group<0>();
         fence_async_smem();
         __syncthreads();
@@ -430,8 +438,11 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 #pragma unroll
             for (int ks = 0; ks < 8; ++ks) {
                 const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
-                const uint64_t bd = smem_desc(bb + ks * 256, 128, 128 * 16);
-                mma_bf16(tmem, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+#pragma unroll
+                for (int j = 0; j < NCH; ++j) {
+                    const uint64_t bd = smem_desc(bb + j * S::CHUNK_BYTES + ks * 256, 128, 128 * 16);
+                    mma_bf16(tmem + j * 9 * WG_NC, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+                }
             }
             mma_commit(&bars[s]);
         }
@@ -469,13 +480,14 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
         // D[co][n], n = tap * 16 + channel: TMEM lane = co (warp w holds lanes 32w..32w+31)
         const int co = co0 + warp * 32 + lane;
 #pragma unroll 1
-        for (int t = 0; t < 9; ++t) {
+        for (int q = 0; q < 9 * NCH; ++q) {   // (chunk, tap)
+            const int j = q / 9, t = q - 9 * j;
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + t * WG_NC, v);
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + q * WG_NC, v);
             if (co < cout) {
-                float *dst = a.dW + ((size_t)co * cin + ci0) * 9 + t;
+                float *dst = a.dW + ((size_t)co * cin + ci0 + WG_NC * j) * 9 + t;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) atomicAdd(dst + 9 * j, v[j]);
+                for (int i = 0; i < 16; ++i) atomicAdd(dst + 9 * i, v[i]);
             }
         }
     }
@@ -487,21 +499,37 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
     }
 }
 
+// One launch over `groups` channel groups of NCH chunks from input channel
+// a.ci_base on, in one wave: the stages fill an SM's shared memory, so one CTA
+// per SM, and the CTAs of every (group, output block) split the tiles evenly,
+// at most kSMs CTAs in all (a last wave of a few CTAs would cost a whole run of
+// tiles).
+template <int NCH>
+int launch_wgrad_tc_t(WgArgs a, int groups, int coblocks, cudaStream_t st)
+{
+    using S = WgSmem<NCH>;
+    const int xctas = std::max(1, kSMs / (groups * coblocks));
+    a.tiles_per_cta = ceil_div(a.n_tiles, xctas);
+    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel<NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
+    const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
+    wgrad_tc_kernel<NCH><<<dim3(ctas, groups, coblocks), WG_TC_THREADS, S::BYTES, st>>>(a);
+    return MVS_OK;
+}
+
 int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, int *err,
                     cudaStream_t st)
 {
     if (cout % 8 || cin % WG_NC) return set_error(MVS_ERR_ARG, "wgrad: cin %d, cout %d", cin, cout);
-    WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0};
+    WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0, 0};
     a.n_tiles = B * a.tiles_x * a.tiles_y;
     const int chunks = cin / WG_NC, coblocks = ceil_div(cout, 128);
-    // one wave: three stages fill an SM's shared memory, so one CTA per SM; the
-    // CTAs of every (chunk, output block) split the tiles evenly, at most kSMs
-    // CTAs in all (a last wave of a few CTAs would cost a whole run of tiles)
-    const int xctas = std::max(1, kSMs / (chunks * coblocks));
-    a.tiles_per_cta = ceil_div(a.n_tiles, xctas);
-    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WgSmem::BYTES));
-    const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
-    wgrad_tc_kernel<<<dim3(ctas, chunks, coblocks), WG_TC_THREADS, WgSmem::BYTES, st>>>(a);
+    // pairs of 16-channel chunks share a staged dz tile; an odd chunk runs alone
+    if (chunks >= 2)
+        if (int rc = launch_wgrad_tc_t<2>(a, chunks / 2, coblocks, st)) return rc;
+    if (chunks & 1) {
+        a.ci_base = (chunks - 1) * WG_NC;
+        if (int rc = launch_wgrad_tc_t<1>(a, 1, coblocks, st)) return rc;
+    }
     return MVS_OK;
 }
 
