@@ -524,9 +524,11 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
     }
 }
 
-// energy_kernel blocks: one pixel per thread, up to this many blocks (then each
-// thread takes several pixels)
-constexpr int kEnergyBlocksMax = 4096;
+// energy_kernel blocks: at most four per SM, each thread taking several pixels.
+// Every block ends with a fence and an increment of one completion counter,
+// which serialise at the counter's L2 slice: 1201 blocks of one pixel per
+// thread at 640x480 spent most of the check there.
+constexpr int kEnergyBlocksMax = 4 * kSMs;
 inline int energy_blocks(int n) { return n / EB + 1 < kEnergyBlocksMax ? n / EB + 1 : kEnergyBlocksMax; }
 
 // ---- persistent iteration: the state stays on chip -----------------------------------
