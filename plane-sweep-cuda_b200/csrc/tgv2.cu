@@ -262,15 +262,137 @@ __device__ __forceinline__ void proj3(double s, double &a, double &b, double &c)
     }
 }
 
-// One full TGV2 iteration (planesweep.cpp:485-509).  The pixel's own operands
-// (r, It, Iu of every view, T, u, u0, v) are loaded before the shared-memory
-// phase so their latency overlaps the halo work.
+// ---- the TGV2 energy (no reference symbol: the reference runs a fixed count) ----
+//
+// alpha1 |T (grad u - v)|_2 + alpha0 |eps(v)| + lambda sum_i |It_i + (u - u0) Iu_i|
+// per pixel, in double, with the forward differences of the P and Q updates
+// (clamped at the last column / row).  `r`, `d` are the right and lower
+// neighbours; `data(du)` adds the views' |It_i + du Iu_i| in view order.
+template <typename DataTerm>
+__device__ __forceinline__ double pixel_energy(float uc, float ur, float ud, float vxc, float vyc, float vxr,
+                                               float vyr, float vxd, float vyd, float t11, float t12, float t22,
+                                               float u0v, double lambda, double alpha0, double alpha1, DataTerm &&data)
+{
+    const double gx = (double)ur - uc - vxc;
+    const double gy = (double)ud - uc - vyc;
+    const double tx = t11 * gx + t12 * gy, ty = t12 * gx + t22 * gy;
+    double ei = alpha1 * sqrt(tx * tx + ty * ty);
+    const double a = (double)vxr - vxc, bb = (double)vyd - vyc;
+    const double c = 0.5 * (((double)vxd - vxc) + ((double)vyr - vyc));
+    ei += alpha0 * sqrt(a * a + bb * bb + 2 * c * c);
+    const double du = (double)uc - u0v;
+    return ei + lambda * data(du);
+}
+
+// Threads of an energy_kernel block (one TX x TY tile).
+constexpr int EB = 256;
+
+// A block's share of the energy, first step (every thread): each warp's sum
+// of `e` into red[warp] (EB / 32 doubles).
+__device__ __forceinline__ void energy_warp_sum(double e, double *red)
+{
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0) red[(threadIdx.x + threadIdx.y * blockDim.x) / 32] = e;
+}
+
+// Second step (thread 0, after a barrier): the warps' sums in warp order,
+// written to partial[block] and fenced before the block counts itself done on
+// the completion counter; true for the block that finished last.
+__device__ __forceinline__ bool energy_block_done(const double *red, double *partial, int block, unsigned nblocks,
+                                                  IterCtl *ctl)
+{
+    double s = 0.0;
+    for (int k = 0; k < EB / 32; ++k) s += red[k];
+    partial[block] = s;
+    __threadfence();   // the partial is visible before the block counts as done
+    return atomicAdd(&ctl->blocks_done, 1u) == nblocks - 1;
+}
+
+// The block that finished last: adds the partial sums in block order, writes
+// the energy and, with tol > 0, applies the stopping test of the launch path
+// (stop_test over the checks of one linearisation); re-arms the counter.
+// Every thread of that block calls it.
+__device__ __forceinline__ void energy_finish(const double *partial, int nblocks, double *red, double *out,
+                                              IterCtl *ctl, double tol, int total, int window)
+{
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    __threadfence();   // every partial is written (each was fenced before its count)
+    double t = 0.0;
+    for (int k = tid; k < nblocks; k += EB) t += __ldcg(partial + k);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if (tid % 32 == 0) red[tid / 32] = t;
+    __syncthreads();
+    if (tid == 0) {
+        double E = 0.0;
+        for (int k = 0; k < EB / 32; ++k) E += red[k];
+        *out = E;
+        if (tol > 0) {
+            if (stop_test(ctl->hist, ctl->n_hist, E, tol, window)) {
+                ctl->done = 1;
+                ctl->stop_total = total;
+            }
+            ++ctl->n_hist;
+            ctl->last_e = E;
+            ctl->have_energy = 1;
+            ctl->energy_at = total;
+        }
+        ctl->blocks_done = 0;   // ready for the next evaluation
+    }
+}
+
+// New p (TGV2_updateP_tensor_weighed_kernel, TGV2_kernels.cu:340-365) and q
+// (TGV2_updateQ_kernel, :54-85) at one cell (rx, ry) of the tile's p/q region,
+// from the ubar / vbar halo in shared memory and the cell's T, p, q operands.
+__device__ __forceinline__ void pq_cell(const float (*sU)[TX + 2], const float (*sVX)[TX + 2],
+                                        const float (*sVY)[TX + 2], float (*sPx)[TX + 1], float (*sPy)[TX + 1],
+                                        float (*sQx)[TX + 1], float (*sQy)[TX + 1], float (*sQz)[TX + 1], int rx,
+                                        int ry, int nx, int ny, float t11, float t12, float t22, float pxin,
+                                        float pyin, float qxin, float qyin, float qzin, float a1s, float a0s)
+{
+    {
+        const double xg = sU[ry][nx] - sU[ry][rx] - sVX[ry][rx];
+        const double yg = sU[ny][rx] - sU[ry][rx] - sVY[ry][rx];
+        const double c11 = t11, c12 = t12, c22 = t22;
+        double dx = (double)pxin + (double)a1s * (c11 * xg + c12 * yg);
+        double dy = (double)pyin + (double)a1s * (c12 * xg + c22 * yg);
+        proj2(dx * dx + dy * dy, dx, dy);
+        sPx[ry][rx] = (float)dx;
+        sPy[ry][rx] = (float)dy;
+    }
+    {
+        const float dx_u1x = sVX[ry][nx] - sVX[ry][rx];
+        const float dy_u1x = sVX[ny][rx] - sVX[ry][rx];
+        const float dx_u1y = sVY[ry][nx] - sVY[ry][rx];
+        const float dy_u1y = sVY[ny][rx] - sVY[ry][rx];
+        double dx = qxin + a0s * dx_u1x;
+        double dy = qyin + a0s * dy_u1y;
+        double dz = qzin + a0s * (dy_u1x + dx_u1y) / 2.0f;
+        proj3(dx * dx + dy * dy + dz * dz + dz * dz, dx, dy, dz);
+        sQx[ry][rx] = (float)dx;
+        sQy[ry][rx] = (float)dy;
+        sQz[ry][rx] = (float)dz;
+    }
+}
+
+// One full TGV2 iteration (planesweep.cpp:485-509).  A 32 x 8 tile computes p
+// and q on the 33 x 9 cells [x0-1, x0+32) x [y0-1, y0+8): thread (tx, ty)
+// takes the cell of its own pixel, threads 0..40 also one of the 41 halo
+// cells (the top row, then the left column).  Every global operand of the
+// iteration -- the pixel's r, It, Iu, T, u, u0, v, p, q, the halo cell's T,
+// p, q and the ubar / vbar halo -- is loaded at the start, one round of loads
+// per CTA; the data duals r and their sum (which read no neighbour) are
+// updated while the halo is stored, so their 3V registers are free before
+// the p / q phase.  The arithmetic and its order are the reference's.
 template <int VMAX>
 __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
 {
     __shared__ float sU[TY + 2][TX + 2], sVX[TY + 2][TX + 2], sVY[TY + 2][TX + 2];
     __shared__ float sPx[TY + 1][TX + 1], sPy[TY + 1][TX + 1];
     __shared__ float sQx[TY + 1][TX + 1], sQy[TY + 1][TX + 1], sQz[TY + 1][TX + 1];
+    constexpr int HALO = (TX + 2) * (TY + 2);    // ubar / vbar halo cells: 340
+    constexpr int HCELLS = TX + 1 + TY;           // p / q cells outside the tile: 41
+    static_assert(HALO <= 2 * TX * TY && HCELLS <= TX * TY, "two halo cells and one p/q halo cell per thread");
     wait_for_previous_grid();   // launched as a dependent launch: the previous iteration is complete
     allow_next_grid();
     if (b.ctl && b.ctl->done) return;   // the run stopped at an earlier energy check
@@ -281,10 +403,10 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     const bool own = x < w && y < h;
     const int i = own ? y * w + x : 0;
     const size_t n = (size_t)w * h;
-
-    // own-pixel operands, prefetched
-    float rv[VMAX], itv[VMAX], iuv[VMAX];
     const int V = b.V;   // <= VMAX (the launch picks VMAX)
+
+    // ---- loads ----
+    float rv[VMAX], itv[VMAX], iuv[VMAX];
 #pragma unroll
     for (int v = 0; v < VMAX; ++v) {
         if (v < V && own) {
@@ -295,6 +417,7 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
         }
     }
     float t11 = 0.f, t12 = 0.f, t22 = 0.f, uold = 0.f, u0v = 0.f, u1xprev = 0.f, u1yprev = 0.f;
+    float pxin = 0.f, pyin = 0.f, qxin = 0.f, qyin = 0.f, qzin = 0.f;
     if (own) {
         t11 = b.T11[i];
         t12 = b.T12[i];
@@ -303,72 +426,88 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
         u0v = b.u0[i];
         u1xprev = b.u1x[i];
         u1yprev = b.u1y[i];
+        pxin = b.Px_in[i];
+        pyin = b.Py_in[i];
+        qxin = b.Qx_in[i];
+        qyin = b.Qy_in[i];
+        qzin = b.Qz_in[i];
     }
-
+    // the halo p / q cell of threads 0..40: (rx, 0) for rx = tid <= TX, then (0, tid - TX)
+    const int hrx = tid <= TX ? tid : 0, hry = tid <= TX ? 0 : tid - TX;
+    const int hpx = x0 - 1 + hrx, hpy = y0 - 1 + hry;
+    const bool hcell = tid < HCELLS && hpx >= 0 && hpy >= 0 && hpx < w && hpy < h;
+    float ht11 = 0.f, ht12 = 0.f, ht22 = 0.f, hpxin = 0.f, hpyin = 0.f, hqxin = 0.f, hqyin = 0.f, hqzin = 0.f;
+    if (hcell) {
+        const int j = hpy * w + hpx;
+        ht11 = b.T11[j];
+        ht12 = b.T12[j];
+        ht22 = b.T22[j];
+        hpxin = b.Px_in[j];
+        hpyin = b.Py_in[j];
+        hqxin = b.Qx_in[j];
+        hqyin = b.Qy_in[j];
+        hqzin = b.Qz_in[j];
+    }
     // ubar, vbar on [x0-1, x0+TX] x [y0-1, y0+TY] (clamped; cells outside the
-    // image are never read)
-    for (int k = tid; k < (TX + 2) * (TY + 2); k += TX * TY) {
-        const int ry = k / (TX + 2), rx = k % (TX + 2);
-        const int px = min(max(x0 - 1 + rx, 0), w - 1), py = min(max(y0 - 1 + ry, 0), h - 1);
-        const int j = py * w + px;
-        sU[ry][rx] = b.ubar_in[j];
-        sVX[ry][rx] = b.u1xbar_in[j];
-        sVY[ry][rx] = b.u1ybar_in[j];
-    }
-    __syncthreads();
-
-    // new p (TGV2_updateP_tensor_weighed_kernel, TGV2_kernels.cu:340-365) and
-    // q (TGV2_updateQ_kernel, :54-85) on [x0-1, x0+TX) x [y0-1, y0+TY)
-    const float a1s = b.alpha1 * b.sigma, a0s = b.alpha0 * b.sigma;
-    for (int k = tid; k < (TX + 1) * (TY + 1); k += TX * TY) {
-        const int ry = k / (TX + 1), rx = k % (TX + 1);
-        const int px = x0 - 1 + rx, py = y0 - 1 + ry;
-        if (px < 0 || py < 0 || px >= w || py >= h) continue;
-        const int j = py * w + px;
-        const int nx = px + 1 <= w - 1 ? rx + 1 : rx, ny = py + 1 <= h - 1 ? ry + 1 : ry;
-        {
-            const double xg = sU[ry][nx] - sU[ry][rx] - sVX[ry][rx];
-            const double yg = sU[ny][rx] - sU[ry][rx] - sVY[ry][rx];
-            const double c11 = b.T11[j], c12 = b.T12[j], c22 = b.T22[j];
-            double dx = (double)b.Px_in[j] + (double)a1s * (c11 * xg + c12 * yg);
-            double dy = (double)b.Py_in[j] + (double)a1s * (c12 * xg + c22 * yg);
-            proj2(dx * dx + dy * dy, dx, dy);
-            sPx[ry][rx] = (float)dx;
-            sPy[ry][rx] = (float)dy;
-        }
-        {
-            const float dx_u1x = sVX[ry][nx] - sVX[ry][rx];
-            const float dy_u1x = sVX[ny][rx] - sVX[ry][rx];
-            const float dx_u1y = sVY[ry][nx] - sVY[ry][rx];
-            const float dy_u1y = sVY[ny][rx] - sVY[ry][rx];
-            double dx = b.Qx_in[j] + a0s * dx_u1x;
-            double dy = b.Qy_in[j] + a0s * dy_u1y;
-            double dz = b.Qz_in[j] + a0s * (dy_u1x + dx_u1y) / 2.0f;
-            proj3(dx * dx + dy * dy + dz * dz + dz * dz, dx, dy, dz);
-            sQx[ry][rx] = (float)dx;
-            sQy[ry][rx] = (float)dy;
-            sQz[ry][rx] = (float)dz;
+    // image are never read): cells tid and tid + TX*TY
+    float hu[2], hvx[2], hvy[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int k = tid + c * TX * TY;
+        hu[c] = hvx[c] = hvy[c] = 0.f;
+        if (k < HALO) {
+            const int ry = k / (TX + 2), rx = k % (TX + 2);
+            const int px = min(max(x0 - 1 + rx, 0), w - 1), py = min(max(y0 - 1 + ry, 0), h - 1);
+            const int j = py * w + px;
+            hu[c] = b.ubar_in[j];
+            hvx[c] = b.u1xbar_in[j];
+            hvy[c] = b.u1ybar_in[j];
         }
     }
-    __syncthreads();
 
-    if (!own) return;
-    const int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
-
-    // r and prodsum (TGV2_updateR_kernel, TGV2_kernels.cu:87-105), views in order
+    // ---- r and prodsum (TGV2_updateR_kernel, TGV2_kernels.cu:87-105), views in order ----
     const float du = uold - u0v;
     const float sl = b.sigma * b.lambda;
     float prodsum = 0.f;
+    if (own) {
 #pragma unroll
-    for (int v = 0; v < VMAX; ++v) {
-        if (v < V) {
-            const float r = proj_unit(rv[v] + sl * (itv[v] + du * iuv[v]));
-            b.r[(size_t)v * n + i] = r;
-            prodsum += r * iuv[v];
+        for (int v = 0; v < VMAX; ++v) {
+            if (v < V) {
+                const float r = proj_unit(rv[v] + sl * (itv[v] + du * iuv[v]));
+                b.r[(size_t)v * n + i] = r;
+                prodsum += r * iuv[v];
+            }
         }
     }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int k = tid + c * TX * TY;
+        if (k < HALO) {
+            const int ry = k / (TX + 2), rx = k % (TX + 2);
+            sU[ry][rx] = hu[c];
+            sVX[ry][rx] = hvx[c];
+            sVY[ry][rx] = hvy[c];
+        }
+    }
+    __syncthreads();
 
-    // primal step (TGV2_updateU_tensor_weighed_kernel, TGV2_kernels.cu:300-338)
+    // ---- p, q on the tile and its left / top halo ----
+    const float a1s = b.alpha1 * b.sigma, a0s = b.alpha0 * b.sigma;
+    const int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
+    if (own) {
+        const int nx = x + 1 <= w - 1 ? lx + 1 : lx, ny = y + 1 <= h - 1 ? ly + 1 : ly;
+        pq_cell(sU, sVX, sVY, sPx, sPy, sQx, sQy, sQz, lx, ly, nx, ny, t11, t12, t22, pxin, pyin, qxin, qyin, qzin,
+                a1s, a0s);
+    }
+    if (hcell) {
+        const int nx = hpx + 1 <= w - 1 ? hrx + 1 : hrx, ny = hpy + 1 <= h - 1 ? hry + 1 : hry;
+        pq_cell(sU, sVX, sVY, sPx, sPy, sQx, sQy, sQz, hrx, hry, nx, ny, ht11, ht12, ht22, hpxin, hpyin, hqxin,
+                hqyin, hqzin, a1s, a0s);
+    }
+    __syncthreads();
+    if (!own) return;
+
+    // ---- primal step (TGV2_updateU_tensor_weighed_kernel, TGV2_kernels.cu:300-338) ----
     const int xp = max(x - 1, 0), yp = max(y - 1, 0);
     const int lxp = lx - (x - xp), lyp = ly - (y - yp);
     const float c_px = sPx[ly][lx], c_py = sPy[ly][lx];
@@ -395,85 +534,46 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     b.Qz_out[i] = qz;
 }
 
-// Energy of the current iterate (the functional the updates minimise; the
-// reference has none): per-block FP64 partial sums, then one block adds them.
-constexpr int EB = 256;
-
-// The TGV2 energy (no reference symbol: the reference runs a fixed count) of
-// the current state: alpha1 |T (grad u - v)|_2 + alpha0 |eps(v)| + lambda
-// sum_i |It_i + (u - u0) Iu_i| per pixel, in double, with the operators of the
-// P, Q and R updates.  Each block adds its pixels' terms; the block that
-// finishes last (a completion counter, nothing waits) adds the blocks' partial
-// sums in block order, writes the energy and, given `ctl`, applies the
-// stopping test of the launch path (stop_test over the checks of one
-// linearisation).  Launches after a met tolerance return at once.
-__global__ void __launch_bounds__(EB) energy_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
-                                                    const float *__restrict__ T22, const float *__restrict__ It,
-                                                    const float *__restrict__ Iu, const float *__restrict__ u0,
-                                                    const float *__restrict__ u, const float *__restrict__ u1x,
-                                                    const float *__restrict__ u1y, int w, int h, int V, double lambda,
-                                                    double alpha0, double alpha1, double *__restrict__ partial,
-                                                    double *__restrict__ out, IterCtl *ctl, double tol, int total,
-                                                    int window)
+// The energy of the current iterate (the energy checks of the launch path and
+// the final energy).  One TX x TY tile per block, one pixel per thread: the
+// iteration's grid, at full occupancy (32 registers), so the pixels' loads
+// are all in flight at once; per warp, then per block in warp order, then
+// the blocks' partial sums in block order by the block that finishes last (a
+// completion counter, nothing waits).  With tol > 0 the last block applies
+// the stopping test.  Launches after a met tolerance return at once.
+__global__ void __launch_bounds__(TX *TY) energy_kernel(const float *__restrict__ T11, const float *__restrict__ T12,
+                                                        const float *__restrict__ T22, const float *__restrict__ It,
+                                                        const float *__restrict__ Iu, const float *__restrict__ u0,
+                                                        const float *__restrict__ u, const float *__restrict__ u1x,
+                                                        const float *__restrict__ u1y, int w, int h, int V,
+                                                        double lambda, double alpha0, double alpha1,
+                                                        double *__restrict__ partial, double *__restrict__ out,
+                                                        IterCtl *ctl, double tol, int total, int window)
 {
     __shared__ double red[EB / 32];
     __shared__ int last;
     wait_for_previous_grid();   // also launched as a dependent launch after the iterations
     allow_next_grid();
     if (ctl->done) return;
-    const int n = w * h;
+    const int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
+    const size_t n = (size_t)w * h;
     double e = 0.0;
-    for (int i = blockIdx.x * EB + threadIdx.x; i < n; i += gridDim.x * EB) {
-        const int y = i / w, x = i - y * w;
-        const int xn = min(x + 1, w - 1), yn = min(y + 1, h - 1);
-        const double gx = (double)u[y * w + xn] - u[i] - u1x[i];
-        const double gy = (double)u[yn * w + x] - u[i] - u1y[i];
-        const double tx = T11[i] * gx + T12[i] * gy, ty = T12[i] * gx + T22[i] * gy;
-        double ei = alpha1 * sqrt(tx * tx + ty * ty);
-        const double a = (double)u1x[y * w + xn] - u1x[i], bb = (double)u1y[yn * w + x] - u1y[i];
-        const double c = 0.5 * (((double)u1x[yn * w + x] - u1x[i]) + ((double)u1y[y * w + xn] - u1y[i]));
-        ei += alpha0 * sqrt(a * a + bb * bb + 2 * c * c);
-        const double du = (double)u[i] - u0[i];
-        double ed = 0.0;
-        for (int v = 0; v < V; ++v) ed += fabs((double)It[(size_t)v * n + i] + du * Iu[(size_t)v * n + i]);
-        e += ei + lambda * ed;
+    if (x < w && y < h) {
+        const int i = y * w + x, jr = y * w + min(x + 1, w - 1), jd = min(y + 1, h - 1) * w + x;
+        e = pixel_energy(u[i], u[jr], u[jd], u1x[i], u1y[i], u1x[jr], u1y[jr], u1x[jd], u1y[jd], T11[i], T12[i],
+                         T22[i], u0[i], lambda, alpha0, alpha1, [&](double du) {
+                             double ed = 0.0;
+                             for (int v = 0; v < V; ++v)
+                                 ed += fabs((double)It[(size_t)v * n + i] + du * Iu[(size_t)v * n + i]);
+                             return ed;
+                         });
     }
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    energy_warp_sum(e, red);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < EB / 32; ++k) s += red[k];
-        partial[blockIdx.x] = s;
-        __threadfence();   // the partial is visible before the block counts as done
-        last = atomicAdd(&ctl->blocks_done, 1u) == gridDim.x - 1;
-    }
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        last = energy_block_done(red, partial, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, ctl);
     __syncthreads();
-    if (!last) return;
-    // the last block: every partial is written (each was fenced before its count)
-    __threadfence();
-    double t = 0.0;
-    for (int k = threadIdx.x; k < (int)gridDim.x; k += EB) t += __ldcg(partial + k);
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double E = 0.0;
-        for (int k = 0; k < EB / 32; ++k) E += red[k];
-        *out = E;
-        if (tol > 0) {
-            if (stop_test(ctl->hist, ctl->n_hist, E, tol, window)) {
-                ctl->done = 1;
-                ctl->stop_total = total;
-            }
-            ++ctl->n_hist;
-            ctl->last_e = E;
-            ctl->have_energy = 1;
-            ctl->energy_at = total;
-        }
-        ctl->blocks_done = 0;   // ready for the next evaluation
-    }
+    if (last) energy_finish(partial, gridDim.x * gridDim.y, red, out, ctl, tol, total, window);
 }
 
 // Dual start for a warm-started primal: one dual step from zero, of size sd
@@ -524,12 +624,6 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
     }
 }
 
-// energy_kernel blocks: at most four per SM, each thread taking several pixels.
-// Every block ends with a fence and an increment of one completion counter,
-// which serialise at the counter's L2 slice: 1201 blocks of one pixel per
-// thread at 640x480 spent most of the check there.
-constexpr int kEnergyBlocksMax = 4 * kSMs;
-inline int energy_blocks(int n) { return n / EB + 1 < kEnergyBlocksMax ? n / EB + 1 : kEnergyBlocksMax; }
 
 // ---- persistent iteration: the state stays on chip -----------------------------------
 //
@@ -943,7 +1037,7 @@ size_t persist_smem_bytes(int th, int V)
 struct Layout {
     float *ref01, *T11, *T12, *T22, *u0, *u1x, *u1y, *ubar[2], *u1xbar[2], *u1ybar[2], *Px[2], *Py[2], *Qx[2],
         *Qy[2], *Qz[2], *It, *Iu, *r;
-    double *partial, *energy;
+    double *partial, *energy;   // energy_kernel's per-block partial sums (one per tile) and result
     IterCtl *ctl;
     float *exb[2], *exq[2], *exu;
     double *ppartial;
@@ -983,7 +1077,7 @@ Layout layout(void *base, int w, int h, int V)
     L.It = take(n * V);
     L.Iu = take(n * V);
     L.r = take(n * V);
-    L.partial = (double *)take(2 * kEnergyBlocksMax);
+    L.partial = (double *)take(2 * (size_t)ceil_div(w, TX) * ceil_div(h, TY));
     L.energy = (double *)take(2);
     L.ctl = (IterCtl *)take(sizeof(IterCtl) / sizeof(float));
     for (int k = 0; k < 2; ++k) {
@@ -1240,6 +1334,106 @@ int tgv2_sparse_run(int w, int h, const float *ref255, const float *depthmap, co
 
 size_t tgv2_workspace_bytes(int w, int h, int V) { return layout(nullptr, w, h, V).bytes; }
 
+// Reads of the stopping flag that do not drain the launch stream.  After each
+// energy check the launch path records an event; once kPollLead more
+// iterations are queued behind it, a side stream waits for that event and
+// copies the flag to the host, so the host learns of a met tolerance while
+// the GPU still has those iterations to run (a copy on the launching stream
+// would wait for all of them, leaving the GPU idle until the next launch
+// arrives).  Iterations queued after a met tolerance return at once.  Only
+// the flag is read this way: the rest of the state is read in stream order at
+// the end of the linearisation.
+constexpr int kPollLead = 20;
+constexpr int kPollRing = 32;
+constexpr int kPollDevices = 64;
+
+// The side stream and events of one device, made on a thread's first checked
+// run on it and kept for the thread's lifetime (making them costs more than a
+// short run's polls save).
+struct PollResources {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev[kPollRing] = {};
+    bool tried = false, ok = false;
+    ~PollResources()
+    {
+        for (int k = 0; k < kPollRing; ++k)
+            if (ev[k]) cudaEventDestroy(ev[k]);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+PollResources *poll_resources()
+{
+    thread_local PollResources res[kPollDevices];
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kPollDevices) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    PollResources &r = res[dev];
+    if (!r.tried) {
+        r.tried = true;
+        r.ok = cudaStreamCreateWithFlags(&r.s, cudaStreamNonBlocking) == cudaSuccess;
+        for (int k = 0; r.ok && k < kPollRing; ++k)
+            r.ok = cudaEventCreateWithFlags(&r.ev[k], cudaEventDisableTiming) == cudaSuccess;
+        if (!r.ok) cudaGetLastError();   // the launch path then polls on its own stream
+    }
+    return r.ok ? &r : nullptr;
+}
+
+struct SidePoll {
+    PollResources *res = nullptr;
+    int at[kPollRing] = {};   // launch count when each check was recorded
+    int head = 0, count = 0;
+    bool ok = false;
+    void open()
+    {
+        res = poll_resources();
+        ok = res != nullptr;
+    }
+    // after a check launch on `st`
+    cudaError_t record(cudaStream_t st, int launched)
+    {
+        const int slot = (head + count) % kPollRing;
+        at[slot] = launched;
+        ++count;
+        return cudaEventRecord(res->ev[slot], st);
+    }
+    // the oldest check's flag, if kPollLead launches are queued behind it (or
+    // the ring is full); `*read` says whether a flag was read
+    cudaError_t due(int launched, const int *d_done, int *h_done, bool *read)
+    {
+        *read = false;
+        if (!count || (launched - at[head] < kPollLead && count < kPollRing)) return cudaSuccess;
+        cudaError_t e = cudaStreamWaitEvent(res->s, res->ev[head], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_done, d_done, sizeof(int), cudaMemcpyDeviceToHost, res->s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(res->s);
+        head = (head + 1) % kPollRing;
+        --count;
+        *read = e == cudaSuccess;
+        return e;
+    }
+    void reset() { head = count = 0; }
+    // a failed side call (say, a context reset since the resources were made):
+    // clear the error, remake them on the next run, poll in order for the rest
+    // of this one
+    void fail()
+    {
+        cudaGetLastError();
+        *res = PollResources{};   // the old handles may be stale: dropped, not destroyed
+        ok = false;
+    }
+};
+
+// One iteration launch for V views (the smallest compiled view count >= V).
+cudaError_t launch_iteration(int V, dim3 grid, dim3 block, cudaStream_t st, const IterBufs &ib)
+{
+    if (V <= 4) return launch_dependent(iteration_kernel<4>, grid, block, 0, st, ib);
+    if (V <= 8) return launch_dependent(iteration_kernel<8>, grid, block, 0, st, ib);
+    if (V <= 16) return launch_dependent(iteration_kernel<16>, grid, block, 0, st, ib);
+    return launch_dependent(iteration_kernel<32>, grid, block, 0, st, ib);
+}
+
 int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, const float *K9, const float *invK9,
              const float *Rrel, const float *trel, const mvs_tgv2_params *prm, int u_from_input, float u_init,
              float *u, int *iters_out, double *energy_out, void *ws, cudaStream_t st, const TGV2Warm *warm)
@@ -1328,8 +1522,12 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
         }
     }
     // launch path: the stopping state lives on the device (IterCtl); the host
-    // reads it every kPoll iterations and at the end of each linearisation
+    // reads its flag after each check (SidePoll; on the launching stream every
+    // kPoll iterations if no side stream could be made) and all of it at the
+    // end of each linearisation
     constexpr int kPoll = 50;
+    SidePoll sp;
+    if (!pth && prm->tol > 0) sp.open();
     IterCtl hc{};
     int launched = 0;
     auto poll = [&]() -> int {
@@ -1450,27 +1648,30 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             ib.Qy_out = L.Qy[cur ^ 1];
             ib.Qz_out = L.Qz[cur ^ 1];
             // dependent launches: each iteration's launch overlaps the previous one's tail
-            if (V <= 4) MVS_TRY_CUDA(launch_dependent(iteration_kernel<4>, gi, bi, 0, st, ib));
-            else if (V <= 8) MVS_TRY_CUDA(launch_dependent(iteration_kernel<8>, gi, bi, 0, st, ib));
-            else if (V <= 16) MVS_TRY_CUDA(launch_dependent(iteration_kernel<16>, gi, bi, 0, st, ib));
-            else MVS_TRY_CUDA(launch_dependent(iteration_kernel<32>, gi, bi, 0, st, ib));
+            MVS_TRY_CUDA(launch_iteration(V, gi, bi, st, ib));
             cur ^= 1;
             ++launched;
-            if (prm->tol > 0 && (k + 1) % check_every == 0) {
-                MVS_TRY_CUDA(launch_dependent(energy_kernel, dim3(energy_blocks(n)), dim3(EB), 0, st, L.T11, L.T12,
-                                              L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V, prm->lambda,
-                                              prm->alpha0, prm->alpha1, L.partial, L.energy, L.ctl, prm->tol,
-                                              launched, stop_window));
-            }
+            const bool check = prm->tol > 0 && (k + 1) % check_every == 0;
+            if (check)
+                MVS_TRY_CUDA(launch_dependent(energy_kernel, gi, bi, 0, st, L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u,
+                                              L.u1x, L.u1y, w, h, V, prm->lambda, prm->alpha0, prm->alpha1, L.partial,
+                                              L.energy, L.ctl, prm->tol, launched, stop_window));
             if (launched >= cap) {
                 done = true;
                 break;
             }
-            if (prm->tol > 0 && launched % kPoll == 0) {
+            if (sp.ok) {
+                cudaError_t e = check ? sp.record(st, launched) : cudaSuccess;
+                bool read = false;
+                if (e == cudaSuccess) e = sp.due(launched, &L.ctl->done, &hc.done, &read);
+                if (e != cudaSuccess) sp.fail();
+                else if (read && hc.done) break;
+            } else if (prm->tol > 0 && launched % kPoll == 0) {
                 if ((rc = poll())) break;
                 if (hc.done) break;
             }
         }
+        sp.reset();
         if (!rc && prm->tol > 0) {
             rc = poll();
             if (!rc && hc.done) {
@@ -1506,9 +1707,8 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
     }
     if (!rc && energy_out && energy_at != total) {
         // energy of the final iterate for callers that ask for it
-        energy_kernel<<<energy_blocks(n), EB, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h,
-                                                      V, prm->lambda, prm->alpha0, prm->alpha1, L.partial, L.energy,
-                                                      L.ctl, 0.0, total, 1);
+        energy_kernel<<<gi, bi, 0, st>>>(L.T11, L.T12, L.T22, L.It, L.Iu, L.u0, u, L.u1x, L.u1y, w, h, V, prm->lambda,
+                                         prm->alpha0, prm->alpha1, L.partial, L.energy, L.ctl, 0.0, total, 1);
         cudaMemcpyAsync(h_energy, L.energy, sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = set_error(MVS_ERR_CUDA, "tgv2 energy: %s", cudaGetErrorString(e));
