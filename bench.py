@@ -681,7 +681,7 @@ def main():
                         "note": "fraction against the HBM model (208 B per pixel); the working set stays in L2 "
                                 "between the back-to-back iterations. The on-chip form (MVS_TGV2_ITER_PERSISTENT) "
                                 "keeps the state in shared memory: 65 MB of DRAM traffic for all 500 iterations, "
-                                "15.9 us per iteration against 14.3 for this form"}
+                                "15.9 us per iteration against 12.8 for this form"}
     sweep_s = statistics.median(sweep_ms) / 1e3
     # algorithmic bytes of the sweep kernel per launch: reference + 8 sources read once,
     # BF16 cost volume written once, WTA partials written once

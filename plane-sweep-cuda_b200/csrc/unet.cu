@@ -345,18 +345,39 @@ struct WgArgs {
     int ci_base;      // first input channel of blockIdx.y == 0
 };
 
-constexpr int WG_TC_THREADS = 128;
+constexpr int WG_TC_THREADS = 256;
 constexpr int WG_NC = 16;                           // input channels per chunk
 constexpr int WG_PLANES = 9 * WG_NC / 8;            // 18 B planes per chunk: (tap, channel group)
 
-template <int NCH>
-struct WgSmem {
-    static constexpr int STAGES = NCH == 1 ? 3 : 2;
-    static constexpr int A_BYTES = 16 * 128 * 16;                // 16 co8 groups x 128 pixels x 16 B
-    static constexpr int CHUNK_BYTES = WG_PLANES * 128 * 16;     // 18 planes x 128 pixels x 16 B
-    static constexpr int STAGE = A_BYTES + NCH * CHUNK_BYTES;
-    static constexpr int BYTES = STAGES * STAGE + 64;
+// Shared memory of wgrad_tc_kernel<NCH, R> for `cg` groups of 8 output
+// channels (cg <= 16):
+//   two MMA buffers, each A = dz [cg][128 pixels][16 B] followed by, per
+//     16-channel chunk, B = the nine tap-shifted input planes
+//     [tap][channel group][128 pixels][16 B] (18 planes);
+//   R raw stages, each the dz tile [cg][128][16 B] and, per chunk, the input
+//     halo [channel group][18 rows][10 columns][16 B], filled by cp.async.
+// The A descriptor of an M = 128 MMA spans 16 groups (32 KB) from A's start;
+// groups past cg read the B planes that follow and only fill accumulator rows
+// co >= cout, which are never stored, so A needs no zero padding.
+constexpr int WG_HALO_W = TW + 2, WG_HALO_H = TH + 2;          // 10 x 18 input pixels around an 8 x 16 tile
+constexpr int WG_HALO_BYTES = 2 * WG_HALO_H * WG_HALO_W * 16;  // per chunk: 5760
+constexpr int WG_PLANES_BYTES = WG_PLANES * 128 * 16;          // per chunk: 36864
+constexpr int WG_SMEM_MAX = 227 * 1024;
+constexpr int WG_SMEM_SM = 228 * 1024;   // shared memory of an SM, 1 KB of it reserved per CTA
+
+struct WgLayout {
+    int a_bytes, buf_bytes, raw_bytes, bytes;
 };
+
+__host__ __device__ inline WgLayout wg_layout(int nch, int stages, int cg)
+{
+    WgLayout L;
+    L.a_bytes = cg * 128 * 16;
+    L.buf_bytes = L.a_bytes + nch * WG_PLANES_BYTES;
+    L.raw_bytes = L.a_bytes + nch * WG_HALO_BYTES;
+    L.bytes = 2 * L.buf_bytes + stages * L.raw_bytes + 64;
+    return L;
+}
 
 // MN-major descriptors have the instruction descriptor's transpose bits set
 __host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) { return idesc_bf16(M, N) | (1u << 15) | (1u << 16); }
@@ -365,16 +386,27 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <int NCH>
+// The weight gradient of a 3x3 convolution on the tensor cores:
+// dW[co][ci][tap] = sum over pixels of dz[co][p] x[ci][p + tap], K = pixels.
+// Per 8 x 16 tile: the raw stage lands (cp.async, R - 1 tiles ahead), the CTA
+// copies its dz tile and expands its input halo into the nine tap-shifted
+// planes of an MMA buffer (shared-memory loads and stores: the input crosses
+// L2 once instead of nine times), and one thread issues 8 K-steps of one
+// MMA of 128 x (9 taps x 16 channels) x 16 pixels per chunk.  The two MMA
+// buffers alternate; a buffer is rebuilt once the MMAs that read it have
+// signalled its mbarrier (tcgen05.commit).  Every wait is bounded.
+template <int NCH, int R>
 __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 {
-    using S = WgSmem<NCH>;
-    constexpr int WG_STAGES = S::STAGES;
+    static_assert(R >= 2, "at least two raw stages");
+    constexpr int NBUF = 2;   // MMA buffers
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = (uint64_t *)(smem + WG_STAGES * S::STAGE);
-    uint32_t *tmem_slot = (uint32_t *)(smem + WG_STAGES * S::STAGE + 32);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ci0 = a.ci_base + blockIdx.y * NCH * WG_NC, co0 = blockIdx.z * 128;
+    const int cg = min(a.cout - co0, 128) >> 3;
+    const WgLayout L = wg_layout(NCH, R, cg);
+    uint64_t *bars = (uint64_t *)(smem + NBUF * L.buf_bytes + R * L.raw_bytes);
+    uint32_t *tmem_slot = (uint32_t *)(smem + NBUF * L.buf_bytes + R * L.raw_bytes + 32);
     const int t_begin = blockIdx.x * a.tiles_per_cta;
     const int t_end = min(t_begin + a.tiles_per_cta, a.n_tiles);
     const int H = a.H, W = a.W, cin = a.cin, cout = a.cout;
@@ -383,90 +415,125 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 
     if (warp == 0) tmem_alloc(tmem_slot, TMEM_COLS);
     if (tid == 0) {
-        for (int k = 0; k < WG_STAGES; ++k) mbar_init(&bars[k], 1);
+        for (int k = 0; k < NBUF; ++k) mbar_init(&bars[k], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // rows co >= cout of A stay zero in every stage
-    for (int k = tid; k < WG_STAGES * S::STAGE / 16; k += WG_TC_THREADS) ((uint4 *)smem)[k] = make_uint4(0, 0, 0, 0);
-    fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t sbase = smem_u32(smem);
+    const uint32_t rbase = sbase + NBUF * L.buf_bytes;
 
-    // cp.async of one tile into stage s (one commit group)
+    // Each thread's copies are the same for every tile: dz pixel (tid & 127) of
+    // the groups tid >> 7, + 2, ...; halo items tid, tid + 256, ... (chunk and
+    // channel group, halo row, halo column), worked out once here.
+    constexpr int HP = WG_HALO_H * WG_HALO_W;
+    constexpr int HALO_ITEMS = NCH * 2 * HP;
+    constexpr int HI = (HALO_ITEMS + WG_TC_THREADS - 1) / WG_TC_THREADS;
+    const int dz_m = tid & 127, dz_y = dz_m >> 3, dz_x = dz_m & 7, dz_g0 = tid >> 7;
+    int h_jg[HI], h_y[HI], h_x[HI];
+#pragma unroll
+    for (int i = 0; i < HI; ++i) {
+        const int k = tid + i * WG_TC_THREADS;
+        const int jg = k / HP, pix = k - jg * HP;
+        h_jg[i] = k < HALO_ITEMS ? jg : -1;
+        h_y[i] = pix / WG_HALO_W - 1;
+        h_x[i] = pix - (pix / WG_HALO_W) * WG_HALO_W - 1;
+    }
+    // cp.async of tile `tile`'s dz and input halo into raw stage s (one commit group)
     auto load = [&](int tile, int s) {
         const int b = tile / (a.tiles_x * a.tiles_y), r = tile - b * a.tiles_x * a.tiles_y;
         const int y0 = (r / a.tiles_x) * TH, x0 = (r % a.tiles_x) * TW;
-        const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
-        const int cg = min(cout - co0, 128) >> 3;
-        for (int k = tid; k < cg * 128; k += WG_TC_THREADS) {
-            const int g = k >> 7, m = k & 127;
-            const int gy = y0 + (m >> 3), gx = x0 + (m & 7);
+        const uint32_t ab = rbase + s * L.raw_bytes, hb = ab + L.a_bytes;
+        const bf16 *xb = a.x + (size_t)b * img * cin + ci0;
+        {
+            const int gy = y0 + dz_y, gx = x0 + dz_x;
             const bool ok = gy < H && gx < W;
-            const bf16 *src = a.dz + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cout + co0 + 8 * g;
-            cp_async16(ab + (g * 128 + m) * 16, src, ok);
+            const bf16 *src = a.dz + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cout + co0 + 8 * dz_g0;
+            for (int g = dz_g0, i = 0; g < cg; g += 2, ++i) cp_async16(ab + (g * 128 + dz_m) * 16, src + 16 * i, ok);
         }
-        for (int k = tid; k < NCH * WG_PLANES * 128; k += WG_TC_THREADS) {
-            const int pl = k >> 7, m = k & 127;          // plane (chunk j, tap t, channel group g), pixel m
-            const int j = pl / WG_PLANES, q = pl - j * WG_PLANES;
-            const int t = q >> 1, g = q & 1, ky = t / 3, kx = t - 3 * ky;
-            const int gy = y0 + (m >> 3) + ky - 1, gx = x0 + (m & 7) + kx - 1;
+#pragma unroll
+        for (int i = 0; i < HI; ++i) {
+            if (h_jg[i] < 0) continue;
+            const int gy = y0 + h_y[i], gx = x0 + h_x[i];
             const bool ok = gy >= 0 && gy < H && gx >= 0 && gx < W;
-            const bf16 *src =
-                a.x + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + ci0 + WG_NC * j + 8 * g;
-            cp_async16(bb + (pl * 128 + m) * 16, src, ok);
+            const bf16 *src = xb + (ok ? (size_t)gy * W + gx : 0) * cin + 8 * h_jg[i];
+            cp_async16(hb + (tid + i * WG_TC_THREADS) * 16, src, ok);
         }
         cp_async_commit();
+    };
+    // raw stage s -> MMA buffer q: the dz tile as is, the halo as nine
+    // tap-shifted planes (thread = tile pixel m and one of the two channel
+    // groups of each chunk, 16 B per plane)
+    auto build = [&](int s, int q) {
+        const uint4 *ra = (const uint4 *)(smem + NBUF * L.buf_bytes + s * L.raw_bytes);
+        const uint4 *rh = ra + L.a_bytes / 16;
+        uint4 *ba = (uint4 *)(smem + q * L.buf_bytes);
+        uint4 *bp = ba + L.a_bytes / 16;
+        for (int k = tid; k < cg * 128; k += WG_TC_THREADS) ba[k] = ra[k];
+        const int m = tid & 127, my = m >> 3, mx = m & 7, g = tid >> 7;
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) {
+            const int jg = 2 * j + g;
+            const uint4 *h = rh + jg * WG_HALO_H * WG_HALO_W;
+            uint4 *dst = bp + j * (WG_PLANES_BYTES / 16) + g * 128 + m;
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const int ky = t / 3, kx = t - 3 * ky;
+                dst[t * 2 * 128] = h[(my + ky) * WG_HALO_W + mx + kx];
+            }
+        }
     };
 
     constexpr uint32_t idesc = idesc_bf16_mn(128, 9 * WG_NC);
     const int n = t_end - t_begin;
     bool failed = false;
     int last = -1;   // the last tile whose MMAs were issued (the same in every thread)
-    for (int k = 0; k < WG_STAGES - 1 && k < n; ++k) load(t_begin + k, k);
+    for (int k = 0; k < R - 1; ++k) {
+        if (k < n) load(t_begin + k, k);
+        else cp_async_commit();   // empty groups keep the group count per tile fixed
+    }
+    // tile c's MMAs read buffer c % NBUF and signal bars[c % NBUF]; that is the
+    // barrier's (c / NBUF)-th completion, of parity (c / NBUF) & 1
     for (int c = 0; c < n; ++c) {
-        const int s = c % WG_STAGES;
-        if (WG_STAGES == 3 && c + 1 < n) cp_async_wait_group<1>();   // tile c landed (c + 1 may be in flight)
-        else cp_async_wait_group<0>();
-        fence_async_smem();
+        const int q = c % NBUF;
+        cp_async_wait_group<R - 2>();   // tile c's group landed (R - 2 newer ones may be in flight)
+        // the MMAs of tile c - NBUF read buffer q
+        const bool ok = c < NBUF || mbar_wait_bounded(&bars[q], (uint32_t)(((c - NBUF) / NBUF) & 1), kWaitNs);
+        // every thread's copies of tile c landed, buffer q is free, raw stage (c - 1) % R is free
+        failed = __syncthreads_or(!ok) != 0;
+        if (failed) break;
+        if (c + R - 1 < n) load(t_begin + c + R - 1, (c + R - 1) % R);
+        else cp_async_commit();
+        build(c % R, q);
+        fence_async_smem();   // the generic-proxy stores, visible to the MMAs
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t ab = sbase + s * S::STAGE, bb = ab + S::A_BYTES;
+            const uint32_t ab = sbase + q * L.buf_bytes, bb = ab + L.a_bytes;
 #pragma unroll
             for (int ks = 0; ks < 8; ++ks) {
                 const uint64_t ad = smem_desc(ab + ks * 256, 128, 128 * 16);
 #pragma unroll
                 for (int j = 0; j < NCH; ++j) {
-                    const uint64_t bd = smem_desc(bb + j * S::CHUNK_BYTES + ks * 256, 128, 128 * 16);
+                    const uint64_t bd = smem_desc(bb + j * WG_PLANES_BYTES + ks * 256, 128, 128 * 16);
                     mma_bf16(tmem + j * 9 * WG_NC, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
                 }
             }
-            mma_commit(&bars[s]);
+            mma_commit(&bars[q]);
         }
         last = c;
-        // refill the stage that tile c - 1's MMAs read once they are done
-        if (c + WG_STAGES - 1 < n) {
-            const int sr = (c + WG_STAGES - 1) % WG_STAGES;
-            if (c >= 1) {
-                const bool ok = mbar_wait_bounded(&bars[sr], (uint32_t)(((c - 1) / WG_STAGES) & 1), kWaitNs);
-                failed = __syncthreads_or(!ok) != 0;
-                if (failed) break;
-            }
-            load(t_begin + c + WG_STAGES - 1, sr);
-        }
     }
     if (!failed && last >= 0) {
-        const bool ok = mbar_wait_bounded(&bars[last % WG_STAGES], (uint32_t)((last / WG_STAGES) & 1), kWaitNs);
+        const bool ok = mbar_wait_bounded(&bars[last % NBUF], (uint32_t)((last / NBUF) & 1), kWaitNs);
         failed = __syncthreads_or(!ok) != 0;
     }
     if (failed) {
         if (tid == 0) atomicExch(a.err, 1);
         cp_async_wait_group<0>();   // copies in flight
         if (last >= 0)              // the MMAs in flight (they complete in order)
-            mbar_wait_bounded(&bars[last % WG_STAGES], (uint32_t)((last / WG_STAGES) & 1), kWaitNs);
+            mbar_wait_bounded(&bars[last % NBUF], (uint32_t)((last / NBUF) & 1), kWaitNs);
         tc_fence_before();
         __syncthreads();
         if (warp == 0) {
@@ -475,15 +542,18 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
         }
         return;
     }
+    cp_async_wait_group<0>();   // the trailing empty groups
     tc_fence_after();
     if (n > 0) {
-        // D[co][n], n = tap * 16 + channel: TMEM lane = co (warp w holds lanes 32w..32w+31)
-        const int co = co0 + warp * 32 + lane;
+        // D[co][n], n = tap * 16 + channel: TMEM lane = co; warps w and w + 4
+        // read lanes 32 (w % 4) .. + 31, the even and the odd (chunk, tap) columns
+        const int quarter = warp & 3;
+        const int co = co0 + quarter * 32 + lane;
 #pragma unroll 1
-        for (int q = 0; q < 9 * NCH; ++q) {   // (chunk, tap)
-            const int j = q / 9, t = q - 9 * j;
+        for (int qq = warp >> 2; qq < 9 * NCH; qq += 2) {   // (chunk, tap)
+            const int j = qq / 9, t = qq - 9 * j;
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + q * WG_NC, v);
+            tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + qq * WG_NC, v);
             if (co < cout) {
                 float *dst = a.dW + ((size_t)co * cin + ci0 + WG_NC * j) * 9 + t;
 #pragma unroll
@@ -500,20 +570,49 @@ __global__ void __launch_bounds__(WG_TC_THREADS) wgrad_tc_kernel(WgArgs a)
 }
 
 // One launch over `groups` channel groups of NCH chunks from input channel
-// a.ci_base on, in one wave: the stages fill an SM's shared memory, so one CTA
-// per SM, and the CTAs of every (group, output block) split the tiles evenly,
-// at most kSMs CTAs in all (a last wave of a few CTAs would cost a whole run of
-// tiles).
-template <int NCH>
-int launch_wgrad_tc_t(WgArgs a, int groups, int coblocks, cudaStream_t st)
+// a.ci_base on, in one wave of `per_sm` CTAs per SM (the buffers fill an SM's
+// shared memory): the CTAs of every (group, output block) split the tiles
+// evenly, at most per_sm * kSMs CTAs in all (a last wave of a few CTAs would
+// cost a whole run of tiles).
+template <int NCH, int R>
+int launch_wgrad_tc_t(WgArgs a, int groups, int coblocks, int per_sm, cudaStream_t st)
 {
-    using S = WgSmem<NCH>;
-    const int xctas = std::max(1, kSMs / (groups * coblocks));
+    const WgLayout L = wg_layout(NCH, R, std::min(a.cout, 128) >> 3);
+    const int xctas = std::max(1, per_sm * kSMs / (groups * coblocks));
     a.tiles_per_cta = ceil_div(a.n_tiles, xctas);
-    MVS_TRY_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel<NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
+    auto kernel = wgrad_tc_kernel<NCH, R>;
+    MVS_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
+    MVS_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
     const int ctas = ceil_div(a.n_tiles, a.tiles_per_cta);
-    wgrad_tc_kernel<NCH><<<dim3(ctas, groups, coblocks), WG_TC_THREADS, S::BYTES, st>>>(a);
+    kernel<<<dim3(ctas, groups, coblocks), WG_TC_THREADS, L.bytes, st>>>(a);
     return MVS_OK;
+}
+
+// Shared memory one CTA may use at `per_sm` CTAs per SM.
+inline int wg_limit(int per_sm) { return per_sm == 1 ? WG_SMEM_MAX : WG_SMEM_SM / per_sm - 1024; }
+
+// The deepest raw ring that fits (at most 8 stages), or 0.
+inline int wg_stages(int nch, int cg, int per_sm)
+{
+    for (int r = 8; r >= 2; --r)
+        if (wg_layout(nch, r, cg).bytes <= wg_limit(per_sm)) return r;
+    return 0;
+}
+
+template <int NCH>
+int launch_wgrad_tc_n(WgArgs a, int groups, int coblocks, int per_sm, cudaStream_t st)
+{
+    switch (wg_stages(NCH, std::min(a.cout, 128) >> 3, per_sm)) {
+    case 8: return launch_wgrad_tc_t<NCH, 8>(a, groups, coblocks, per_sm, st);
+    case 7: return launch_wgrad_tc_t<NCH, 7>(a, groups, coblocks, per_sm, st);
+    case 6: return launch_wgrad_tc_t<NCH, 6>(a, groups, coblocks, per_sm, st);
+    case 5: return launch_wgrad_tc_t<NCH, 5>(a, groups, coblocks, per_sm, st);
+    case 4: return launch_wgrad_tc_t<NCH, 4>(a, groups, coblocks, per_sm, st);
+    case 3: return launch_wgrad_tc_t<NCH, 3>(a, groups, coblocks, per_sm, st);
+    case 2: return launch_wgrad_tc_t<NCH, 2>(a, groups, coblocks, per_sm, st);
+    default: return set_error(MVS_ERR_ARG, "wgrad: %d chunks do not fit", NCH);
+    }
 }
 
 int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int H, int W, float *dW, int *err,
@@ -523,12 +622,21 @@ int launch_wgrad_tc(const bf16 *x, int cin, const bf16 *dz, int cout, int B, int
     WgArgs a{x, dz, dW, err, B, H, W, cin, cout, ceil_div(W, TW), ceil_div(H, TH), 1, 0, 0};
     a.n_tiles = B * a.tiles_x * a.tiles_y;
     const int chunks = cin / WG_NC, coblocks = ceil_div(cout, 128);
-    // pairs of 16-channel chunks share a staged dz tile; an odd chunk runs alone
-    if (chunks >= 2)
-        if (int rc = launch_wgrad_tc_t<2>(a, chunks / 2, coblocks, st)) return rc;
-    if (chunks & 1) {
-        a.ci_base = (chunks - 1) * WG_NC;
-        if (int rc = launch_wgrad_tc_t<1>(a, 1, coblocks, st)) return rc;
+    const int cg = std::min(cout, 128) >> 3;
+    // Two CTAs per SM, one chunk each, where one chunk's buffers and at least
+    // three raw stages fit in half an SM (16 output channels): the two CTAs'
+    // barrier-separated phases overlap.  Otherwise one CTA per SM: pairs of
+    // 16-channel chunks share a staged dz tile where two chunks' buffers and
+    // two raw stages fit, and an odd chunk runs alone.  (A single MMA buffer
+    // to fit two CTAs per SM at 32 and 64 output channels measured no faster.)
+    if (wg_stages(1, cg, 2) >= 3) return launch_wgrad_tc_n<1>(a, chunks, coblocks, 2, st);
+    const bool pairs = chunks >= 2 && wg_stages(2, cg, 1) >= 2;
+    if (pairs)
+        if (int rc = launch_wgrad_tc_n<2>(a, chunks / 2, coblocks, 1, st)) return rc;
+    const int first = pairs ? chunks & ~1 : 0;
+    if (first < chunks) {
+        a.ci_base = first * WG_NC;
+        if (int rc = launch_wgrad_tc_n<1>(a, chunks - first, coblocks, 1, st)) return rc;
     }
     return MVS_OK;
 }
