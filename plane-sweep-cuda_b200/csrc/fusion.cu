@@ -182,6 +182,39 @@ __device__ __forceinline__ float prox_median(const uint32_t *cnt, float u, float
     return fminf(fmaxf(uc, lo), hi);
 }
 
+// The U step of one voxel (FusionUpdateU_kernel, fusion.cu:45-57): u + tau
+// div p, the histogram proximal median, and v = 2 u_new - u_old.
+template <int BINS>
+__device__ __forceinline__ float u_step(float div, float u_old, const uint32_t *cnt, double tau, float tl, float &v_new)
+{
+    const double un = u_old;
+    const double uu = un - tau * (-(double)div);
+    const float m = prox_median<BINS>(cnt, (float)uu, tl);
+    v_new = (float)((double)(2 * m) - un);
+    return m;
+}
+
+// The P step of one voxel (FusionUpdateP_kernel, fusion.cu:59-70): p + sigma
+// grad v with the forward differences of gradVFwd (fusion.h:773-781, zero at
+// the far faces: hx, hy, hz say whether the +x, +y, +z neighbour exists),
+// then projectUnitBall (fusion.h:866-870; dividing by exactly 1 is the identity).
+__device__ __forceinline__ void p_step(float px, float py, float pz, float vi, float vx1, float vy1, float vz1, bool hx,
+                                       bool hy, bool hz, float sigma, float &qx, float &qy, float &qz)
+{
+    const float gx = hx ? vx1 - vi : 0.f;
+    const float gy = hy ? vy1 - vi : 0.f;
+    const float gz = hz ? vz1 - vi : 0.f;
+    qx = px + sigma * gx;
+    qy = py + sigma * gy;
+    qz = pz + sigma * gz;
+    const float d = fmaxf(1.f, sqrtf(qx * qx + qy * qy + qz * qz));
+    if (d != 1.f) {
+        qx = qx / d;
+        qy = qy / d;
+        qz = qz / d;
+    }
+}
+
 template <int BINS>
 __global__ void __launch_bounds__(VX *VY) update_u_kernel(Dims D, const uint16_t *__restrict__ hist,
                                                          float *__restrict__ u, float *__restrict__ v,
@@ -201,13 +234,11 @@ __global__ void __launch_bounds__(VX *VY) update_u_kernel(Dims D, const uint16_t
     if (x > 0) div -= px[i - 1];
     if (y > 0) div -= py[i - D.vw];
     if (z > 0) div -= pz[i - sz];
-    const double un = u[i];
-    const double uu = un - tau * (-(double)div);
     uint32_t cnt[HS];
     load_counts<HS>(hist, (long)i, cnt);
-    const float m = prox_median<BINS>(cnt, (float)uu, tl);
-    u[i] = m;
-    v[i] = (float)((double)(2 * m) - un);
+    float vn;
+    u[i] = u_step<BINS>(div, u[i], cnt, tau, tl, vn);
+    v[i] = vn;
 }
 
 __global__ void __launch_bounds__(VX *VY) update_p_kernel(Dims D, const float *__restrict__ v, float *__restrict__ p,
@@ -220,19 +251,11 @@ __global__ void __launch_bounds__(VX *VY) update_p_kernel(Dims D, const float *_
     const size_t sz = (size_t)D.vw * D.vh, n = sz * D.vd;
     const size_t i = (size_t)z * sz + (size_t)y * D.vw + x;
     float *px = p, *py = p + n, *pz = p + 2 * n;
+    const bool hx = x < D.vw - 1, hy = y < D.vh - 1, hz = z < D.vd - 1;
     const float vi = v[i];
-    // gradVFwd (fusion.h:773-781): zero at the far faces
-    const float gx = x < D.vw - 1 ? v[i + 1] - vi : 0.f;
-    const float gy = y < D.vh - 1 ? v[i + D.vw] - vi : 0.f;
-    const float gz = z < D.vd - 1 ? v[i + sz] - vi : 0.f;
-    float qx = px[i] + sigma * gx, qy = py[i] + sigma * gy, qz = pz[i] + sigma * gz;
-    // projectUnitBall (fusion.h:866-870); dividing by exactly 1 is the identity
-    const float d = fmaxf(1.f, sqrtf(qx * qx + qy * qy + qz * qz));
-    if (d != 1.f) {
-        qx = qx / d;
-        qy = qy / d;
-        qz = qz / d;
-    }
+    float qx, qy, qz;
+    p_step(px[i], py[i], pz[i], vi, hx ? v[i + 1] : 0.f, hy ? v[i + D.vw] : 0.f, hz ? v[i + sz] : 0.f, hx, hy, hz,
+           sigma, qx, qy, qz);
     px[i] = qx;
     py[i] = qy;
     pz[i] = qz;
