@@ -320,20 +320,18 @@ int launch_conv(const bf16 *in, int cin, const bf16 *wpack, const float *bias, c
 // ---------------------------------------------------------------------------
 // weight gradient on tensor cores: for every tap t = (ky, kx),
 //   D[co][t][ci] += sum_p dz[p][co] * x[p + off_t][ci]
-// with K = pixels, for 16-channel chunks of the input.  A = dz^T (M = co,
-// padded to 128 rows of zeros) and B = the nine tap-shifted copies of the
-// input tile (N = 9 taps x 16 channels = 144) are both MN-major with the same
-// layout, [8-group][pixel][8]: A as [co/8][pixel][8], B as
-// [tap][ci/8][pixel][8] where plane (t, g) holds x at the tile's pixels
-// shifted by tap t's offset.  One K step of 16 pixels (two tile rows) is then
-// a single MMA for all nine taps (8 per tile, with N = 144), instead of one
-// MMA per tap (72 with N = 16).  A CTA takes NCH = 1 or 2 chunks (16 or 32
-// input channels) against one staged dz tile: NCH MMAs per K step into NCH
-// accumulators.  Tiles stream through a cp.async pipeline of three stages
-// (NCH = 1) or two (NCH = 2), each stage's copies one commit group; an
-// mbarrier signalled by tcgen05.commit says when a stage's MMAs are done and
-// it may be refilled.  Each CTA sums a run of pixel tiles in TMEM (144 NCH
-// columns) and adds them to the FP32 gradient with one atomic per weight.
+// with K = pixels, for 16-channel chunks of the input.  A = dz^T (M = co, up
+// to 128 rows) and B = the nine tap-shifted copies of the input tile (N = 9
+// taps x 16 channels = 144) are both MN-major with the same layout,
+// [8-group][pixel][8]: A as [co/8][pixel][8], B as [tap][ci/8][pixel][8] where
+// plane (t, g) holds x at the tile's pixels shifted by tap t's offset.  One K
+// step of 16 pixels (two tile rows) is then a single MMA for all nine taps (8
+// per tile, with N = 144), instead of one MMA per tap (72 with N = 16).  A CTA
+// takes NCH = 1 or 2 chunks (16 or 32 input channels) against one staged dz
+// tile: NCH MMAs per K step into NCH accumulators.  The tap planes are built
+// in shared memory from the tile's input halo (wgrad_tc_kernel below); each
+// CTA sums a run of pixel tiles in TMEM (144 NCH columns) and adds them to the
+// FP32 gradient with one atomic per weight.
 // ---------------------------------------------------------------------------
 
 struct WgArgs {
