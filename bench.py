@@ -643,12 +643,13 @@ def main():
     # the caller's host images: the reference and one (V, H, W) array of sources
     h_ref = np.ascontiguousarray(fr.ref, dtype=np.float32)
     h_srcs = np.ascontiguousarray(np.stack(fr.srcs), dtype=np.float32)
+    h_depth = np.empty((H, W), np.float32)   # the caller's depthmap, filled every frame
 
     def e2e_step():
         ps.set_reference(h_ref, fr.ref_cam.R, fr.ref_cam.t)
         ps.set_sources(h_srcs, Rsrc, tsrc)
         ps.RunAlgorithm()
-        return ps.getDepthmap()
+        return ps.getDepthmap(out=h_depth)
 
     for _ in range(args.warmup):
         e2e_step()

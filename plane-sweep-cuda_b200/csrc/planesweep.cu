@@ -11,6 +11,9 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <new>
 #include <thread>
 #include <vector>
@@ -92,6 +95,70 @@ struct CopyPiece {
 // threads wait on each other in the driver: 44 calls for an 11 MB frame).
 constexpr size_t kUploadChunk = (size_t)1 << 20;
 
+// Worker threads for parallel_copy, made on first use and kept for the
+// process (spawning seven threads for every frame cost more than the copies
+// they shared).  A job is fn(0 .. parts-1): the caller and the workers claim
+// parts from one counter, and the caller returns once every worker has
+// checked in for that job, so none still holds it.  The pool is never
+// destroyed (its workers wait on it until the process ends).
+class CopyPool {
+public:
+    static CopyPool *get()
+    {
+        static CopyPool *pool = new CopyPool(std::min(7u, std::max(1u, std::thread::hardware_concurrency()) - 1));
+        return pool;
+    }
+    int workers() const { return nworkers_; }
+    // false if another caller holds the pool (that caller's job is not shared)
+    bool try_run(int parts, const std::function<void(int)> &fn)
+    {
+        std::unique_lock<std::mutex> busy(busy_, std::try_to_lock);
+        if (!busy.owns_lock()) return false;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            fn_ = &fn;
+            parts_ = parts;
+            next_.store(0);
+            pending_ = nworkers_;
+            ++gen_;
+        }
+        work_.notify_all();
+        for (int k; (k = next_.fetch_add(1)) < parts;) fn(k);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+        fn_ = nullptr;
+        return true;
+    }
+
+private:
+    explicit CopyPool(int n) : nworkers_(n)
+    {
+        for (int k = 0; k < n; ++k) std::thread([this] { loop(); }).detach();
+    }
+    void loop()
+    {
+        unsigned long long seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            work_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            const std::function<void(int)> *fn = fn_;
+            const int parts = parts_;
+            lk.unlock();
+            for (int k; (k = next_.fetch_add(1)) < parts;) (*fn)(k);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    const int nworkers_;
+    std::mutex busy_, mu_;
+    std::condition_variable work_, done_;
+    const std::function<void(int)> *fn_ = nullptr;
+    int parts_ = 0, pending_ = 0;
+    unsigned long long gen_ = 0;
+    std::atomic<int> next_{0};
+};
+
 // Returns 0, or the first CUDA error of a queued upload.
 int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
 {
@@ -101,7 +168,13 @@ int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int parts = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total / min_part));
     std::atomic<int> err{0};
+    // uploads queued from other threads go to the caller's device (a thread
+    // starts on device 0), so stream 0 there is the caller's stream 0
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const std::thread::id caller = std::this_thread::get_id();
     auto run = [&](int k) {
+        if (std::this_thread::get_id() != caller) cudaSetDevice(dev);
         // part k copies bytes [k * total / parts, (k + 1) * total / parts) of the concatenation
         const size_t lo = total * k / parts, hi = total * (k + 1) / parts;
         size_t base = 0;
@@ -126,6 +199,8 @@ int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
         run(0);
         return err.load();
     }
+    const std::function<void(int)> job = run;
+    if (CopyPool *pool = CopyPool::get(); pool->workers() >= parts - 1 && pool->try_run(parts, job)) return err.load();
     std::vector<std::thread> th;
     th.reserve(parts - 1);
     for (int k = 1; k < parts; ++k) th.emplace_back(run, k);

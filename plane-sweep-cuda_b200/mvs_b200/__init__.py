@@ -797,30 +797,35 @@ class PlaneSweep:
         check(_L.mvs_ps_tgv_ext(self.h, C.byref(params), start, _fp(ui), C.byref(it), C.byref(e)))
         return it.value, e.value
 
-    def _img(self, name, dtype=np.float32):
-        # every element is written: the library refuses a map of another size
-        out = np.empty(self.shape, dtype)
+    def _img(self, name, dtype=np.float32, out=None):
+        # every element is written: the library refuses a map of another size.
+        # `out`: a C-contiguous array of the frame's shape and type to fill (a
+        # caller that keeps one avoids a fresh allocation per frame)
+        if out is None:
+            out = np.empty(self.shape, dtype)
+        elif out.dtype != dtype or out.shape != tuple(self.shape) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous {np.dtype(dtype).name} array of shape {tuple(self.shape)}")
         ptr = out.ctypes.data_as(_F if dtype == np.float32 else _U8)
         check(getattr(_L, f"mvs_ps_get_{name}")(self.h, ptr))
         return out
 
-    def getDepthmap(self):
-        return self._img("depthmap")
+    def getDepthmap(self, out=None):
+        return self._img("depthmap", out=out)
 
-    def getDepthmap8u(self):
-        return self._img("depthmap8u", np.uint8)
+    def getDepthmap8u(self, out=None):
+        return self._img("depthmap8u", np.uint8, out)
 
-    def getDepthmapDenoised(self):
-        return self._img("depthmap_denoised")
+    def getDepthmapDenoised(self, out=None):
+        return self._img("depthmap_denoised", out=out)
 
-    def getDepthmap8uDenoised(self):
-        return self._img("depthmap8u_denoised", np.uint8)
+    def getDepthmap8uDenoised(self, out=None):
+        return self._img("depthmap8u_denoised", np.uint8, out)
 
-    def getDepthmapTGV(self):
-        return self._img("depthmap_tgv")
+    def getDepthmapTGV(self, out=None):
+        return self._img("depthmap_tgv", out=out)
 
-    def getDepthmap8uTGV(self):
-        return self._img("depthmap8u_tgv", np.uint8)
+    def getDepthmap8uTGV(self, out=None):
+        return self._img("depthmap8u_tgv", np.uint8, out)
 
     def getDepthmapDenoisedPtr(self):
         p = _VP()
