@@ -47,6 +47,16 @@ def test_run_algorithm_bit_exact(cuda, golden, name, from_list):
     zn, zf = np.float32(g["znear"]), np.float32(g["zfar"])
     want8 = np.where(d == d, (np.float32(255) * np.clip((d - zn) / (zf - zn), 0, 1)).astype(np.uint8), 255)
     np.testing.assert_array_equal(ps.getDepthmap8u(), want8.astype(np.uint8))
+    # a caller's buffer is filled in place; one of another shape or type is refused
+    buf = np.full(g["depth"].shape, -1.0, np.float32)
+    assert ps.getDepthmap(out=buf) is buf
+    np.testing.assert_array_equal(buf, g["depth"])
+    buf8 = np.zeros(g["depth"].shape, np.uint8)
+    np.testing.assert_array_equal(ps.getDepthmap8u(out=buf8), want8.astype(np.uint8))
+    with pytest.raises(ValueError):
+        ps.getDepthmap(out=np.empty(g["depth"].shape, np.float64))
+    with pytest.raises(ValueError):
+        ps.getDepthmap(out=np.empty((3, 3), np.float32))
 
 
 def test_denoise_tgv_and_points_follow_the_reference(cuda, golden):
