@@ -68,6 +68,11 @@ __global__ void tensor_kernel(const float *__restrict__ ref255, int w, int h, fl
     }
 }
 
+// The per-view arrays r, It and Iu are stored view-interleaved, [pixel][VS]
+// with VS = V rounded up to a multiple of 4, so a pixel's views are whole
+// 16-byte words (the padding entries are never used).
+__host__ __device__ constexpr int view_stride(int V) { return (V + 3) & ~3; }
+
 // Start of a linearisation (planesweep.cpp:445-458,482): u0 = ubar = u, the
 // other primal/dual variables and r to zero.
 __global__ void warp_init_kernel(int n, int V, const float *__restrict__ u, float *__restrict__ u0,
@@ -82,7 +87,8 @@ __global__ void warp_init_kernel(int n, int V, const float *__restrict__ u, floa
         ubar[i] = v;
         u1x[i] = u1y[i] = u1xbar[i] = u1ybar[i] = 0.f;
         Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
-        for (int k = 0; k < V; ++k) r[(size_t)k * n + i] = 0.f;
+        const int VS = view_stride(V);
+        for (int k = 0; k < VS; ++k) r[(size_t)i * VS + k] = 0.f;
     }
 }
 
@@ -112,8 +118,18 @@ __global__ void warm_init_kernel(int n, int V, const float *__restrict__ u_lin, 
         } else {
             Px[i] = Py[i] = Qx[i] = Qy[i] = Qz[i] = 0.f;
         }
-        for (int k = 0; k < V; ++k) r[(size_t)k * n + i] = r_in ? r_in[(size_t)k * n + i] : 0.f;
+        // r_in: the caller's [V][n] planes
+        const int VS = view_stride(V);
+        for (int k = 0; k < VS; ++k) r[(size_t)i * VS + k] = r_in && k < V ? r_in[(size_t)k * n + i] : 0.f;
     }
+}
+
+// view-interleaved r ([pixel][VS]) to [V][n] planes
+__global__ void r_planes_kernel(const float *__restrict__ r, int n, int V, float *__restrict__ out)
+{
+    const int VS = view_stride(V);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int v = 0; v < V; ++v) out[(size_t)v * n + i] = r[(size_t)i * VS + v];
 }
 
 __global__ void fill_kernel(float *__restrict__ p, int n, float v)
@@ -182,8 +198,9 @@ __global__ void linearize_kernel(Cams c, const float *__restrict__ srcs255, cons
     const float dfx = fx * (dX * Z - X * dZ) / (Z * Z);
     const float dfy = fy * (dY * Z - Y * dZ) / (Z * Z);
     const double gx = Ixn - Iw, gy = Iyn - Iw;
-    Iu[(size_t)v * n + i] = (float)(gx * (double)dfx + gy * (double)dfy);
-    It[(size_t)v * n + i] = Iw - ref01[i];
+    const int VS = view_stride((int)gridDim.z);   // one grid layer per view
+    Iu[(size_t)i * VS + v] = (float)(gx * (double)dfx + gy * (double)dfy);
+    It[(size_t)i * VS + v] = Iw - ref01[i];
 }
 
 // Stopping state of a launch-per-iteration run, in device memory.  The energy
@@ -402,18 +419,23 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool own = x < w && y < h;
     const int i = own ? y * w + x : 0;
-    const size_t n = (size_t)w * h;
     const int V = b.V;   // <= VMAX (the launch picks VMAX)
 
     // ---- loads ----
+    const int VS = view_stride(V);
     float rv[VMAX], itv[VMAX], iuv[VMAX];
+    if (own) {
+        const float4 *r4 = reinterpret_cast<const float4 *>(b.r + (size_t)i * VS);
+        const float4 *t4 = reinterpret_cast<const float4 *>(b.It + (size_t)i * VS);
+        const float4 *d4 = reinterpret_cast<const float4 *>(b.Iu + (size_t)i * VS);
 #pragma unroll
-    for (int v = 0; v < VMAX; ++v) {
-        if (v < V && own) {
-            const size_t k = (size_t)v * n + i;
-            rv[v] = b.r[k];
-            itv[v] = b.It[k];
-            iuv[v] = b.Iu[k];
+        for (int q = 0; q < VMAX / 4; ++q) {
+            if (4 * q < V) {
+                const float4 a = r4[q], c = t4[q], d = d4[q];
+                rv[4 * q] = a.x, rv[4 * q + 1] = a.y, rv[4 * q + 2] = a.z, rv[4 * q + 3] = a.w;
+                itv[4 * q] = c.x, itv[4 * q + 1] = c.y, itv[4 * q + 2] = c.z, itv[4 * q + 3] = c.w;
+                iuv[4 * q] = d.x, iuv[4 * q + 1] = d.y, iuv[4 * q + 2] = d.z, iuv[4 * q + 3] = d.w;
+            }
         }
     }
     float t11 = 0.f, t12 = 0.f, t22 = 0.f, uold = 0.f, u0v = 0.f, u1xprev = 0.f, u1yprev = 0.f;
@@ -470,14 +492,20 @@ __global__ void __launch_bounds__(TX *TY) iteration_kernel(IterBufs b)
     const float sl = b.sigma * b.lambda;
     float prodsum = 0.f;
     if (own) {
+        float rn[VMAX];
 #pragma unroll
         for (int v = 0; v < VMAX; ++v) {
+            rn[v] = 0.f;
             if (v < V) {
                 const float r = proj_unit(rv[v] + sl * (itv[v] + du * iuv[v]));
-                b.r[(size_t)v * n + i] = r;
+                rn[v] = r;
                 prodsum += r * iuv[v];
             }
         }
+        float4 *r4 = reinterpret_cast<float4 *>(b.r + (size_t)i * VS);
+#pragma unroll
+        for (int q = 0; q < VMAX / 4; ++q)
+            if (4 * q < V) r4[q] = make_float4(rn[4 * q], rn[4 * q + 1], rn[4 * q + 2], rn[4 * q + 3]);
     }
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -556,15 +584,23 @@ __global__ void __launch_bounds__(TX *TY) energy_kernel(const float *__restrict_
     allow_next_grid();
     if (ctl->done) return;
     const int x = blockIdx.x * TX + threadIdx.x, y = blockIdx.y * TY + threadIdx.y;
-    const size_t n = (size_t)w * h;
     double e = 0.0;
     if (x < w && y < h) {
         const int i = y * w + x, jr = y * w + min(x + 1, w - 1), jd = min(y + 1, h - 1) * w + x;
         e = pixel_energy(u[i], u[jr], u[jd], u1x[i], u1y[i], u1x[jr], u1y[jr], u1x[jd], u1y[jd], T11[i], T12[i],
                          T22[i], u0[i], lambda, alpha0, alpha1, [&](double du) {
                              double ed = 0.0;
-                             for (int v = 0; v < V; ++v)
-                                 ed += fabs((double)It[(size_t)v * n + i] + du * Iu[(size_t)v * n + i]);
+                             // the pixel's views as 16-byte words, added in view order
+                             const int VS = view_stride(V);
+                             const float4 *t4 = reinterpret_cast<const float4 *>(It + (size_t)i * VS);
+                             const float4 *d4 = reinterpret_cast<const float4 *>(Iu + (size_t)i * VS);
+                             for (int q = 0; 4 * q < V; ++q) {
+                                 const float4 a = t4[q], c = d4[q];
+                                 const float tv[4] = {a.x, a.y, a.z, a.w}, dv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+                                 for (int e = 0; e < 4; ++e)
+                                     if (4 * q + e < V) ed += fabs((double)tv[e] + du * dv[e]);
+                             }
                              return ed;
                          });
     }
@@ -593,7 +629,6 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
-    const size_t n = (size_t)w * h;
     const int i = y * w + x, xn = min(x + 1, w - 1), yn = min(y + 1, h - 1);
     const int ix = y * w + xn, iy = yn * w + x;
     if (do_pq) {
@@ -618,7 +653,7 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
     if (!do_r) return;
     const float du = u[i] - u0[i];
     for (int v = 0; v < V; ++v) {
-        const size_t k = (size_t)v * n + i;
+        const size_t k = (size_t)i * view_stride(V) + v;
         float q = sdr * lambda * (It[k] + du * Iu[k]);
         r[k] = q / fmaxf(1.f, fabsf(q));
     }
@@ -759,7 +794,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
         sT11[k] = b.T11[i];
         sT12[k] = b.T12[i];
         sT22[k] = b.T22[i];
-        for (int v = 0; v < V; ++v) sR[v * NP + k] = b.r[(size_t)v * n + i];
+        for (int v = 0; v < V; ++v) sR[v * NP + k] = b.r[(size_t)i * view_stride(V) + v];
     }
     __syncthreads();
 
@@ -885,8 +920,8 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
 #pragma unroll
             for (int v = 0; v < PT_VMAX; ++v) {
                 if (v < V) {
-                    itv[v] = __ldg(b.It + (size_t)v * n + i);
-                    iuv[v] = __ldg(b.Iu + (size_t)v * n + i);
+                    itv[v] = __ldg(b.It + (size_t)i * view_stride(V) + v);
+                    iuv[v] = __ldg(b.Iu + (size_t)i * view_stride(V) + v);
                 }
             }
             const float u0v = __ldg(b.u0 + i);
@@ -963,8 +998,8 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
 #pragma unroll
                 for (int v = 0; v < PT_VMAX; ++v) {
                     if (v < V) {
-                        itv[v] = __ldg(b.It + (size_t)v * n + i);
-                        iuv[v] = __ldg(b.Iu + (size_t)v * n + i);
+                        itv[v] = __ldg(b.It + (size_t)i * view_stride(V) + v);
+                        iuv[v] = __ldg(b.Iu + (size_t)i * view_stride(V) + v);
                     }
                 }
                 const double du = (double)uc - __ldg(b.u0 + i);
@@ -1013,7 +1048,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
             b.Qx[i] = sQx[QI(ly, lx)];
             b.Qy[i] = sQy[QI(ly, lx)];
             b.Qz[i] = sQz[QI(ly, lx)];
-            for (int v = 0; v < V; ++v) b.r[(size_t)v * n + i] = sR[v * NP + q];
+            for (int v = 0; v < V; ++v) b.r[(size_t)i * view_stride(V) + v] = sR[v * NP + q];
         }
     }
     if (blockIdx.x == 0 && tid == 0) {
@@ -1074,9 +1109,9 @@ Layout layout(void *base, int w, int h, int V)
         L.Qy[k] = take(n);
         L.Qz[k] = take(n);
     }
-    L.It = take(n * V);
-    L.Iu = take(n * V);
-    L.r = take(n * V);
+    L.It = take(n * view_stride(V));   // [pixel][VS] (view_stride)
+    L.Iu = take(n * view_stride(V));
+    L.r = take(n * view_stride(V));
     L.partial = (double *)take(2 * (size_t)ceil_div(w, TX) * ceil_div(h, TY));
     L.energy = (double *)take(2);
     L.ctl = (IterCtl *)take(sizeof(IterCtl) / sizeof(float));
@@ -1701,8 +1736,8 @@ int tgv2_run(int w, int h, int V, const float *ref255, const float *srcs255, con
             cudaMemcpyAsync(warm->pq + (size_t)k * n, src[k], n * sizeof(float), cudaMemcpyDeviceToDevice, st);
         rc = check_launch("tgv2 dual readout");
     }
-    if (!rc && warm && warm->r) {
-        cudaMemcpyAsync(warm->r, L.r, (size_t)V * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (!rc && warm && warm->r) {   // the caller's [V][n] planes
+        r_planes_kernel<<<eg, 256, 0, st>>>(L.r, n, V, warm->r);
         rc = check_launch("tgv2 dual readout");
     }
     if (!rc && energy_out && energy_at != total) {
