@@ -7,6 +7,7 @@
 // host; device buffers are kept across calls and only grow.
 #include <math.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -100,7 +101,9 @@ constexpr size_t kUploadChunk = (size_t)1 << 20;
 // they shared).  A job is fn(0 .. parts-1): the caller and the workers claim
 // parts from one counter, and the caller returns once every worker has
 // checked in for that job, so none still holds it.  The pool is never
-// destroyed (its workers wait on it until the process ends).
+// destroyed (its workers wait on it until the process ends).  A process
+// forked after the pool was made has none of its threads, so it does not use
+// it.
 class CopyPool {
 public:
     static CopyPool *get()
@@ -109,9 +112,11 @@ public:
         return pool;
     }
     int workers() const { return nworkers_; }
-    // false if another caller holds the pool (that caller's job is not shared)
+    // false if another caller holds the pool (that caller's job is not
+    // shared), or in a process forked after the pool was made
     bool try_run(int parts, const std::function<void(int)> &fn)
     {
+        if (getpid() != owner_) return false;
         std::unique_lock<std::mutex> busy(busy_, std::try_to_lock);
         if (!busy.owns_lock()) return false;
         {
@@ -131,7 +136,7 @@ public:
     }
 
 private:
-    explicit CopyPool(int n) : nworkers_(n)
+    explicit CopyPool(int n) : nworkers_(n), owner_(getpid())
     {
         for (int k = 0; k < n; ++k) std::thread([this] { loop(); }).detach();
     }
@@ -151,6 +156,7 @@ private:
         }
     }
     const int nworkers_;
+    const pid_t owner_;
     std::mutex busy_, mu_;
     std::condition_variable work_, done_;
     const std::function<void(int)> *fn_ = nullptr;
