@@ -606,11 +606,15 @@ def main():
         # algorithmic HBM bytes per voxel: histogram 32 (16-byte counts in and out);
         # one iteration = U (p 12, u 4, counts 16 in; u 4, v 4 out) + P (v 4, p 12 in; p 12 out) = 68
         tv_gbs = nvox * 68 * fiters / tv_s / 1e9
+        # compulsory bytes of an iteration that moves each array once (u 4, p 12, 7 uint16
+        # counts 14 in; u 4, p 12 out): 46, the lower bound the two passes are held against
+        tv_gbs46 = nvox * 46 * fiters / tv_s / 1e9
         fusion = {"workload": f"{args.fusion_dims}^3 voxels, 40 maps 640x480, 7 bins, 200 TV-L1 iterations",
                   "histogram_voxel_updates_per_s": nvox * 40 * ws / hist_s, "histogram_ms": hist_s * 1e3,
                   "tvl1_voxel_iterations_per_s": nvox * fiters * ws / tv_s, "tvl1_ms": tv_s * 1e3,
                   "tvl1_roofline": {"bound": "hbm", "achieved": tv_gbs, "peak": peaks()[0], "unit": "GB/s",
-                                    "frac": tv_gbs / peaks()[0], "bytes_per_voxel_iteration": 68}}
+                                    "frac": tv_gbs / peaks()[0], "bytes_per_voxel_iteration": 68,
+                                    "frac_of_compulsory_46B": tv_gbs46 / peaks()[0]}}
 
     if fusion is not None and rank == 0 and ws == 1 and not args.no_cpu_baseline:
         # the reference's own fusion kernels on the host cores (oracle/_ref, OpenMP over
