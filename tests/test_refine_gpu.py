@@ -50,6 +50,26 @@ def test_tgv2_bit_exact_vs_reference(cuda, golden, name):
     np.testing.assert_array_equal(u, g["u"])
 
 
+@pytest.mark.parametrize("n_views", [5, 10])
+def test_tgv2_view_counts_with_padded_stride_bit_exact(cuda, n_views):
+    """The per-view duals and linearisation are stored [pixel][V rounded up to
+    4]: 5 views (stride 8, kernel for up to 8 views) and 10 (stride 12, kernel
+    for up to 16) equal the oracle's f32 run, which follows the reference's
+    arithmetic, bit for bit."""
+    fr, planes, win = scenes.config_tiny(seed=9, width=72, height=40, n_src=n_views, n_planes=8, win=5)
+    poses = [(c.R, c.t) for c in fr.src_cams]
+    K1 = fr.ref_cam.K_1based
+    g = dict(K=np.float32(K1), Rref=fr.ref_cam.R, tref=fr.ref_cam.t, Rsrc=np.stack([c.R for c in fr.src_cams]),
+             tsrc=np.stack([c.t for c in fr.src_cams]))
+    K9, iK9, Rs, ts = tgv_inputs(g)
+    u0 = fr.depth_gt.astype(np.float32)
+    u, it, _ = run_tgv(cuda, fr.ref, fr.srcs, K9, iK9, Rs, ts, M.tgv2_params(niters=6, warps=2), u0)
+    assert it == 12
+    uo, _, _ = po.tgv2(fr.ref, fr.srcs, K1, fr.ref_cam.R, fr.ref_cam.t, poses, niters=6, warps=2, u_init=u0,
+                       precision="f32")
+    np.testing.assert_array_equal(u, uo)
+
+
 def test_tgv2_anisotropic_tensor_vs_reference(cuda, golden):
     """beta = 1.5, gamma = 0.8: the anisotropic diffusion tensor
     (TGV2_kernels.cu:257-298) weights the P step and the divergence of the U
