@@ -660,6 +660,25 @@ __global__ void dual_init_kernel(const float *__restrict__ T11, const float *__r
 }
 
 
+// A pixel's It and Iu of views 0 .. V-1 (view-interleaved, view_stride) as
+// 16-byte words.
+template <int VMAX>
+__device__ __forceinline__ void load_views(const float *__restrict__ It, const float *__restrict__ Iu, size_t i, int V,
+                                           float *itv, float *iuv)
+{
+    const int VS = view_stride(V);
+    const float4 *t4 = reinterpret_cast<const float4 *>(It + i * VS);
+    const float4 *d4 = reinterpret_cast<const float4 *>(Iu + i * VS);
+#pragma unroll
+    for (int q = 0; q < VMAX / 4; ++q) {
+        if (4 * q < V) {
+            const float4 c = __ldg(t4 + q), d = __ldg(d4 + q);
+            itv[4 * q] = c.x, itv[4 * q + 1] = c.y, itv[4 * q + 2] = c.z, itv[4 * q + 3] = c.w;
+            iuv[4 * q] = d.x, iuv[4 * q + 1] = d.y, iuv[4 * q + 2] = d.z, iuv[4 * q + 3] = d.w;
+        }
+    }
+}
+
 // ---- persistent iteration: the state stays on chip -----------------------------------
 //
 // One CTA per SM owns a 64 x TH tile for a whole linearisation: u, v, their
@@ -917,13 +936,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
             const size_t i = (size_t)y * w + x;
             // this pixel's L2 operands, all requested before the first use
             float itv[PT_VMAX], iuv[PT_VMAX];
-#pragma unroll
-            for (int v = 0; v < PT_VMAX; ++v) {
-                if (v < V) {
-                    itv[v] = __ldg(b.It + (size_t)i * view_stride(V) + v);
-                    iuv[v] = __ldg(b.Iu + (size_t)i * view_stride(V) + v);
-                }
-            }
+            load_views<PT_VMAX>(b.It, b.Iu, i, V, itv, iuv);
             const float u0v = __ldg(b.u0 + i);
             const float uold = sU[UI(ly, lx)], u1xprev = sVx[UI(ly, lx)], u1yprev = sVy[UI(ly, lx)];
             const float du = uold - u0v;
@@ -995,13 +1008,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) tgv2_persistent_kernel(PersistB
                 const double cc = 0.5 * (((double)sVx[UI(lyn, lx)] - vxc) + ((double)sVy[UI(ly, lxn)] - vyc));
                 ei += b.dalpha0 * sqrt(a * a + bb * bb + 2 * cc * cc);
                 float itv[PT_VMAX], iuv[PT_VMAX];
-#pragma unroll
-                for (int v = 0; v < PT_VMAX; ++v) {
-                    if (v < V) {
-                        itv[v] = __ldg(b.It + (size_t)i * view_stride(V) + v);
-                        iuv[v] = __ldg(b.Iu + (size_t)i * view_stride(V) + v);
-                    }
-                }
+                load_views<PT_VMAX>(b.It, b.Iu, i, V, itv, iuv);
                 const double du = (double)uc - __ldg(b.u0 + i);
                 double ed = 0.0;
 #pragma unroll
