@@ -170,7 +170,8 @@ int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
 {
     size_t total = 0;
     for (const CopyPiece &c : pieces) total += c.bytes;
-    const size_t min_part = (size_t)1 << 20;
+    // a part of at least 256 KB: a 640x480 float image is shared by four threads
+    const size_t min_part = (size_t)1 << 18;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int parts = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total / min_part));
     std::atomic<int> err{0};
@@ -938,7 +939,8 @@ static int copy_image(const mvs_planesweep *ps, const CamImage<T> *img, T *out)
     if (!out) return mvs::set_error(MVS_ERR_ARG, "null output");
     if (!img || img->empty()) return mvs::set_error(MVS_ERR_STATE, "no such depthmap yet");
     if (int rc = frame_check(ps, img->width(), img->height(), "depthmap")) return rc;
-    memcpy(out, img->data(), sizeof(T) * img->elements());
+    // the pool's threads share a large copy; nothing is uploaded
+    mvs::parallel_copy({{out, img->data(), sizeof(T) * img->elements(), nullptr}}, 0);
     return MVS_OK;
 }
 }

@@ -176,9 +176,12 @@ __device__ __forceinline__ constexpr float flat_kappa()
 
 // Reference moments of the tile, once per CTA: in REFERENCE mode the mean and
 // the naive std (calculate_STD_kernel, kernels.cu:103-120) of the reference
-// window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2 (0 if flat).
+// window; in COMPENSATED mode the shifted sum and n*Syy - Sy^2 (0 if flat),
+// or +inf where that is below (st n)^2: the reference window's std is under
+// the threshold, and ncc_of's rsqrt(n^2 var_w * inf) = 0 then gives NCC 0
+// without a test per view and plane (st > 0; with st = 0 nothing changes).
 template <int WIN, int MOM, int TWS = 0>
-__device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float (*RM)[CSP],
+__device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], float shift, float st, float (*RM)[CSP],
                             float (*RS)[CSP])
 {
     using G = Geo<WIN, TWS>;
@@ -222,8 +225,10 @@ __device__ void ref_moments(const float (*Rt)[RWMAX], float (*CS)[TH][CSP], floa
             RS[y][x + j] = var > 0 ? sqrtf(var) : 0.f;
         } else {
             const float v = fmaf(-m[j], m[j], (float)(WIN * WIN) * q[j]);   // n^2 * var
+            const float rs = v > flat_kappa<WIN, TWS>() * q[j] ? v : 0.f;
+            const float thr = st * (float)(WIN * WIN);
             RM[y][x + j] = m[j];
-            RS[y][x + j] = v > flat_kappa<WIN, TWS>() * q[j] ? v : 0.f;
+            RS[y][x + j] = rs >= thr * thr ? rs : INFINITY;
         }
     }
     __syncthreads();
@@ -242,7 +247,9 @@ __device__ __forceinline__ float ncc_of(float s1, float s2, float s12, float rm,
         const float vx = fmaf(-s1, s1, n * s2);         // n^2 var_w
         const float cv = fmaf(-s1, rm, n * s12);        // n^2 cov
         const float thr = st * n;                        // std >= st  <=>  n^2 var >= (st n)^2
-        if (!(vx >= thr * thr) || !(rs >= thr * thr) || !(vx > flat_kappa<WIN, TWS>() * s2)) return 0.f;
+        // rs is +inf where the reference window is under the threshold
+        // (ref_moments): vx > 0 here, so the product is +inf and the NCC 0
+        if (!(vx >= thr * thr) || !(vx > flat_kappa<WIN, TWS>() * s2)) return 0.f;
         return cv * rsqrtf(vx * rs);
     }
 }
@@ -280,9 +287,19 @@ __device__ __forceinline__ void ncc_run(const float *s1, const float *s2, const 
 struct __align__(16) Smem {
     float Wt[RHMAX][RWMAX];        // warped region (reference region at start)
     float CS[3][TH][CSP];          // column sums
-    float Hm[2][9];                // homographies of this and the next (plane, view)
+    float Hm[2][12];               // homographies of this and the next (plane, view): 9 used, 16-byte rows
     float red[THREADS / 32];
 };
+
+// the nine elements of a homography row of Smem::Hm: three 16-byte loads
+__device__ __forceinline__ void load_hm(const float *row, float *Hm)
+{
+    const float4 a = reinterpret_cast<const float4 *>(row)[0], b = reinterpret_cast<const float4 *>(row)[1];
+    const float c = row[8];
+    Hm[0] = a.x, Hm[1] = a.y, Hm[2] = a.z, Hm[3] = a.w;
+    Hm[4] = b.x, Hm[5] = b.y, Hm[6] = b.z, Hm[7] = b.w;
+    Hm[8] = c;
+}
 
 template <int WIN, int MOM, int TWS = 0>
 __device__ __forceinline__ void load_ref_region(Smem &S, const float *__restrict__ ref, int w, int h, int x0,
@@ -340,7 +357,8 @@ struct __align__(16) AggSmem {
 // three CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
 static_assert(3 * (sizeof(AggSmem) + 1024) <= 228 * 1024, "three CTAs per SM");
 static_assert(offsetof(AggSmem, RM) % 16 == 0 && offsetof(AggSmem, RS) % 16 == 0 &&
-                  offsetof(AggSmem, S.CS) % 16 == 0 && (CSP * sizeof(float)) % 16 == 0,
+                  offsetof(AggSmem, S.CS) % 16 == 0 && offsetof(AggSmem, S.Hm) % 16 == 0 &&
+                  (CSP * sizeof(float)) % 16 == 0,
               "16-byte run loads");
 
 // Each source pixel's 2x2 bilinear neighbourhood (x, x+1 on rows y, y+1) as
@@ -582,7 +600,7 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    ref_moments<WIN, MOM, TWS>(S.Wt, S.CS, shift, A.RM, A.RS);
+    ref_moments<WIN, MOM, TWS>(S.Wt, S.CS, shift, a.stdthresh, A.RM, A.RS);
     const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
 
     const int ly = b_row(), lx = b_seg() * G::RUN;
@@ -610,8 +628,7 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
         for (int j = 0; j < G::RUN; ++j) acc[j] = 0.f;
         for (int view = 0; view < a.V; ++view) {
             float Hm[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[hb][k];
+            load_hm(S.Hm[hb], Hm);
             const bool last_view = view + 1 == a.V;
             const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
             float hn = 0.f;
@@ -702,7 +719,7 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, a.stdthresh, A.RM, A.RS);
     const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
     const int ly = b_row(), lx = b_seg() * G::RUN;
     const float sh = MOM == MVS_MOMENTS_REFERENCE ? 0.f : shift;
@@ -722,8 +739,7 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_view_kernel(SweepArgs a)
     int hb = 0;
     for (int p = p0; p < p1; ++p) {
         float Hm[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Hm[k] = S.Hm[hb][k];
+        load_hm(S.Hm[hb], Hm);
         float hn = 0.f;
         if (threadIdx.x < 9 && p + 1 < p1) hn = ldg(Hv + (size_t)(p + 1) * 9 + threadIdx.x);
         if (quad)
@@ -975,7 +991,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_tma_kernel(SweepA
         const float r = rx < G::RW ? S.Wt[ry][rx] : 0.f;
         A.Rf[ry][rx] = (MOM == MVS_MOMENTS_REFERENCE) ? r : r - shift;
     }
-    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, A.RM, A.RS);
+    ref_moments<WIN, MOM>(S.Wt, S.CS, shift, a.stdthresh, A.RM, A.RS);
     const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
     const int ly = b_row(), lx = b_seg() * G::RUN;
     const int y = y0 + ly, xb = x0 + lx;
@@ -994,8 +1010,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_tma_kernel(SweepA
         for (int j = 0; j < G::RUN; ++j) acc[j] = 0.f;
         for (int view = 0; view < a.V; ++view, ++k) {
             float Hm[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) Hm[i] = S.Hm[hb][i];
+            load_hm(S.Hm[hb], Hm);
             const bool last_view = view + 1 == a.V;
             const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
             float hn = 0.f;
