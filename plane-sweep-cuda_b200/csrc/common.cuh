@@ -93,6 +93,15 @@ __device__ __forceinline__ uint16_t f2bf(float f)
     return (uint16_t)(u >> 16);
 }
 
+// f2bf for a value that is not NaN: the hardware's round-to-nearest-even
+// conversion, one instruction, the same bits as f2bf for every other input.
+__device__ __forceinline__ uint16_t f2bf_num(float f)
+{
+    uint16_t b;
+    asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(b) : "f"(f));
+    return b;
+}
+
 __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

@@ -152,9 +152,9 @@ __device__ __forceinline__ void row_sums(const float (*CSq)[CSP], float *out)
             out[j] = m / (float)WIN;
         }
     } else {
-        float m = 0.f;
+        float m = v[0];
 #pragma unroll
-        for (int i = 0; i < WIN; ++i) m += v[i];
+        for (int i = 1; i < WIN; ++i) m += v[i];
         out[0] = m;
 #pragma unroll
         for (int j = 1; j < G::RUN; ++j) {
@@ -558,9 +558,11 @@ __device__ __forceinline__ void pass_a1_rows(const float (*Wt)[RWMAX], float (*C
         float rf[G::SROWS];
 #pragma unroll
         for (int i = 0; i < G::SROWS; ++i) rf[i] = Rf[r0 + i][c];
-        float s1 = 0.f, s2 = 0.f, s12 = 0.f;
+        // the window's first term starts the sums (0 + x is x, up to the sign
+        // of a zero sum, which no NCC sees)
+        float s1 = wv[0], s2 = wv[0] * wv[0], s12 = rf[0] * wv[0];
 #pragma unroll
-        for (int i = 0; i < WIN; ++i) {
+        for (int i = 1; i < WIN; ++i) {
             s1 += wv[i];
             s2 = fmaf(wv[i], wv[i], s2);
             s12 = fmaf(rf[i], wv[i], s12);
@@ -656,7 +658,7 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             // below 0; the stored bf16 bits then order like unsigned integers)
             float cf = fmaf(-acc[j], invV, 1.f);
             cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
-            cb[j] = f2bf(cf);
+            cb[j] = f2bf_num(cf);   // cf is not NaN here
             best[j] = min(best[j], ((uint32_t)cb[j] << 16) | (uint32_t)p);
         }
         if (a.cost && y < h) {
@@ -1054,7 +1056,7 @@ __global__ void __launch_bounds__(THREADS, 2) sweep_aggregated_tma_kernel(SweepA
         for (int j = 0; j < G::RUN; ++j) {
             float cf = fmaf(-acc[j], invV, 1.f);
             cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
-            cb[j] = f2bf(cf);
+            cb[j] = f2bf_num(cf);   // cf is not NaN here
             best[j] = min(best[j], ((uint32_t)cb[j] << 16) | (uint32_t)p);
         }
         if (a.cost && y < h) {
