@@ -237,23 +237,30 @@ struct PlaneSweepImpl {
     int n_views = 0, n_planes = 0, w = 0, h = 0;
     // Images that the C-ABI setters (the only writers of the host images of a
     // handle) uploaded while staging them: RunAlgorithm then uploads neither.
-    // `uploaded` marks the end of those copies; the host images are not
-    // rewritten or freed before it.
+    // `uploaded[0]` marks the end of the reference image's copies and
+    // `uploaded[1]` that of the sources': each host image is not rewritten or
+    // freed before its own event (so the sources are staged while the
+    // reference is still on its way).
     bool ref_dev = false;
     int srcs_dev = 0, dev_w = 0, dev_h = 0;
-    cudaEvent_t uploaded = nullptr;
+    cudaEvent_t uploaded[2] = {nullptr, nullptr};
+    // the plane depths on the device (RunAlgorithm uploads them when they change)
+    std::vector<float> dev_planes;
     PlaneSweepImpl()
     {
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        if (cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming) != cudaSuccess) uploaded = nullptr;
+        for (cudaEvent_t &e : uploaded)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) e = nullptr;
     }
+    bool can_upload() const { return uploaded[0] && uploaded[1]; }
     ~PlaneSweepImpl()
     {
-        if (uploaded) {
-            cudaEventSynchronize(uploaded);
-            cudaEventDestroy(uploaded);
-        }
+        for (cudaEvent_t e : uploaded)
+            if (e) {
+                cudaEventSynchronize(e);
+                cudaEventDestroy(e);
+            }
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
     }
@@ -372,8 +379,14 @@ bool PlaneSweep::RunAlgorithm(int, char **)
         if (cudaMemcpyAsync(I.srcs.as<float>() + v * n, HostSrc[v].data(), n * 4, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             goto cuda_fail;
-    if (cudaMemcpyAsync(I.depths.p, planes.data(), (size_t)P * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        goto cuda_fail;
+    // a pageable copy may wait for the uploads queued before it: only when the
+    // planes change (the buffer grows only for more planes, which differ)
+    if (planes != I.dev_planes) {
+        I.dev_planes.clear();
+        if (cudaMemcpyAsync(I.depths.p, planes.data(), (size_t)P * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            goto cuda_fail;
+        I.dev_planes = planes;
+    }
     {
         cudaEventRecord(I.e0, st);
         if (fp64homography) {
@@ -729,7 +742,7 @@ int mvs_ps_set_reference(mvs_planesweep *ps, const float *img, int32_t w, int32_
     PlaneSweepImpl &I = *ps->ps.impl;
     // the previous uploads still read the host images (no event: no device,
     // the images stay on the host for RunAlgorithm)
-    if (I.uploaded) cudaEventSynchronize(I.uploaded);
+    if (I.uploaded[0]) cudaEventSynchronize(I.uploaded[0]);
     const size_t bytes = sizeof(float) * (size_t)w * h;
     ps->ps.HostRef.reset(w, h);
     ps->ps.HostRef.R = Matrix3D(R9);
@@ -738,9 +751,9 @@ int mvs_ps_set_reference(mvs_planesweep *ps, const float *img, int32_t w, int32_
     if (w != I.dev_w || h != I.dev_h) I.srcs_dev = 0;
     // staged and uploaded together (RunAlgorithm's stream); a failed upload
     // leaves the image to RunAlgorithm
-    const bool up = I.uploaded && I.ref.ensure(bytes) == MVS_OK;
+    const bool up = I.can_upload() && I.ref.ensure(bytes) == MVS_OK;
     const int rc = mvs::parallel_copy({{ps->ps.HostRef.data(), img, bytes, up ? I.ref.p : nullptr}}, 0);
-    if (up && rc == 0 && cudaEventRecord(I.uploaded, 0) == cudaSuccess) {
+    if (up && rc == 0 && cudaEventRecord(I.uploaded[0], 0) == cudaSuccess) {
         I.ref_dev = true;
         I.dev_w = w;
         I.dev_h = h;
@@ -755,10 +768,10 @@ int mvs_ps_set_sources(mvs_planesweep *ps, const float *imgs, int32_t n, const f
     if (w == 0) return mvs::set_error(MVS_ERR_STATE, "set the reference image first");
     if (n < 0 || (n > 0 && (!imgs || !R9s || !t3s))) return mvs::set_error(MVS_ERR_ARG, "bad source images");
     PlaneSweepImpl &I = *ps->ps.impl;
-    if (I.uploaded) cudaEventSynchronize(I.uploaded);
+    if (I.uploaded[1]) cudaEventSynchronize(I.uploaded[1]);
     const size_t bytes = sizeof(float) * (size_t)w * h;
     I.srcs_dev = 0;
-    const bool up = I.uploaded && n > 0 && I.srcs.ensure(bytes * n) == MVS_OK;
+    const bool up = I.can_upload() && n > 0 && I.srcs.ensure(bytes * n) == MVS_OK;
     ps->ps.HostSrc.resize(n);
     std::vector<mvs::CopyPiece> pieces;
     for (int v = 0; v < n; ++v) {
@@ -769,7 +782,7 @@ int mvs_ps_set_sources(mvs_planesweep *ps, const float *imgs, int32_t n, const f
         ps->ps.HostSrc[v].t = Vector3D(t3s + 3 * v);
     }
     const int rc = mvs::parallel_copy(pieces, 0);
-    if (up && rc == 0 && cudaEventRecord(I.uploaded, 0) == cudaSuccess) {
+    if (up && rc == 0 && cudaEventRecord(I.uploaded[1], 0) == cudaSuccess) {
         I.srcs_dev = n;
         I.dev_w = w;
         I.dev_h = h;

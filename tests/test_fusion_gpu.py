@@ -69,15 +69,24 @@ def test_fusion_vs_fp64_oracle(cuda):
     assert np.quantile(err, 0.999) <= 1e-4 and err.max() <= 1e-3, (np.quantile(err, 0.999), err.max())
 
 
-def test_prox_median_matches_insertion_sort(cuda):
+def prox_want(hist, u0, bins, tau, lam):
+    L = po.oracle_lib()
+    return np.array([L.orc_prox_hist_f32(bins, np.ascontiguousarray(hist[:, i]).ctypes.data_as(po._U16),
+                                         float(np.float32(np.float64(u0[i]))), np.float32(tau), np.float32(lam))
+                     for i in range(hist.shape[1])], np.float32)
+
+
+@pytest.mark.parametrize("bins,top", [(7, 12), (7, 4000), (10, 12), (10, 4000)])
+def test_prox_median_matches_insertion_sort(cuda, bins, top):
     """The closed-form median of the U kernel against sortedHist's insertion (structs.h:241-262):
-    random histograms and start values, u read back after one U step with p = 0."""
+    random histograms and start values, u read back after one U step with p = 0.  Counts up to
+    12 (and 200 in a few voxels), and up to 4000: the volume counts in 16 bits."""
     import torch
     rng = np.random.default_rng(3)
-    dims, bins = (16, 8, 8), 7
+    dims = (16, 8, 8)
     n = dims[0] * dims[1] * dims[2]
     vol = M.FusionVolume(dims, bins, [0, 0, 0], [1, 1, 1])
-    hist = rng.integers(0, 12, size=(bins, n)).astype(np.uint16)
+    hist = rng.integers(0, top, size=(bins, n)).astype(np.uint16)
     hist[:, :50] = 0
     hist[0, 50:60] = 200
     u0 = rng.uniform(-3, 3, n).astype(np.float32)
@@ -86,11 +95,57 @@ def test_prox_median_matches_insertion_sort(cuda):
     vol.update_u(tau, lam)
     torch.cuda.synchronize()
     r = vol.download()
-    L = po.oracle_lib()
-    want = np.array([L.orc_prox_hist_f32(bins, np.ascontiguousarray(hist[:, i]).ctypes.data_as(po._U16),
-                                         float(np.float32(np.float64(u0[i]))), np.float32(tau), np.float32(lam))
-                     for i in range(n)], np.float32)
-    np.testing.assert_array_equal(r["u"], want)
+    np.testing.assert_array_equal(r["u"], prox_want(hist, u0, bins, tau, lam))
+
+
+class _DeviceArray:
+    """A device pointer of the library as an array that torch can wrap without a copy."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
+                                         "strides": None, "version": 3}
+
+
+def test_counts_written_through_device_pointer(cuda):
+    """Counts written by the caller through mvs_fusion_device_state's pointer reach the next U
+    step (counts below 40, then one count of 300), and after a reset and a histogram pass the U
+    step reads that pass's counts."""
+    import torch
+    rng = np.random.default_rng(5)
+    dims, bins = (16, 8, 8), 7
+    n = dims[0] * dims[1] * dims[2]
+    vol = M.FusionVolume(dims, bins, [0, 0, 0], [1, 1, 1])
+    u0 = rng.uniform(-3, 3, n).astype(np.float32)
+    zeros = dict(v=np.zeros(n, np.float32), p=np.zeros((3, n), np.float32))
+    tau, lam = 0.1, 0.5
+    st = vol.device_state()
+    hs = st["hist_stride"]
+    for top in (40, 300):
+        hist = rng.integers(0, 40, size=(bins, n)).astype(np.uint16)
+        hist[2, 77] = top
+        dev = np.zeros((n, hs), np.uint16)
+        dev[:, :bins] = hist.T
+        vol.upload(u=u0, **zeros)
+        st = vol.device_state()
+        view = torch.as_tensor(_DeviceArray(st["hist"], (n, hs), "<i2"), device=cuda)
+        view.copy_(torch.from_numpy(dev.view(np.int16)).to(cuda))
+        torch.cuda.synchronize()
+        vol.update_u(tau, lam)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(vol.download()["u"], prox_want(hist, u0, bins, tau, lam))
+    vol.reset()
+    fi = scenes.fusion_sequence(9, 2, 96, 72)
+    vol.set_volume(fi.vol_min, fi.vol_max)
+    Ks = np.stack([c.K for c in fi.cams]).astype(np.float32)
+    Rs = np.stack([c.R for c in fi.cams]).astype(np.float32)
+    ts = np.stack([c.t for c in fi.cams]).astype(np.float32)
+    vol.histogram(torch.from_numpy(np.stack(fi.depths)).to(cuda), Ks, Rs, ts, 0.05)
+    vol.upload(u=u0, **zeros)
+    vol.update_u(tau, lam)
+    torch.cuda.synchronize()
+    r = vol.download()
+    assert r["hist"].sum() > 0
+    np.testing.assert_array_equal(r["u"], prox_want(r["hist"], u0, bins, tau, lam))
 
 
 def test_extract_surface_points(cuda):
