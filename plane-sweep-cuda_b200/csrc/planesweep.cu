@@ -216,6 +216,37 @@ int parallel_copy(const std::vector<CopyPiece> &pieces, cudaStream_t st = 0)
     return err.load();
 }
 
+// True when the host range [p, p + bytes) starts and ends in page-locked
+// memory (cudaHostAlloc'd or registered), which the copy engine reads
+// directly: then one copy of the whole range beats staging it.
+bool page_locked(const void *p, size_t bytes)
+{
+    for (const void *q : {p, (const void *)((const char *)p + bytes - 1)}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();   // not a pointer the runtime knows: pageable
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
+// A caller's page-locked images: one upload of the whole range from the
+// caller's memory on stream 0, while the pool threads copy the same bytes
+// into the handle's host images (`pieces`, concatenated in order, nothing
+// uploaded from them).  Returns once both are done, so the caller may reuse
+// its memory; true if the upload was made (else the images stay on the host
+// for RunAlgorithm).
+bool direct_upload(void *dev, const void *src, size_t bytes, const std::vector<CopyPiece> &pieces, cudaEvent_t done)
+{
+    const bool up = cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, 0) == cudaSuccess;
+    parallel_copy(pieces, 0);
+    const bool ok = up && cudaEventRecord(done, 0) == cudaSuccess && cudaEventSynchronize(done) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    return ok;
+}
+
 // ConvertDepthtoUChar (planesweep.cpp:279-290) per pixel, for the sweep
 // result while it is still on the device: the same float division, clamp
 // and truncation, so the bytes equal the host conversion's.
@@ -749,9 +780,18 @@ int mvs_ps_set_reference(mvs_planesweep *ps, const float *img, int32_t w, int32_
     ps->ps.HostRef.t = Vector3D(t3);
     I.ref_dev = false;
     if (w != I.dev_w || h != I.dev_h) I.srcs_dev = 0;
-    // staged and uploaded together (RunAlgorithm's stream); a failed upload
+    // staged and uploaded together (RunAlgorithm's stream), or uploaded from
+    // the caller's page-locked image while it is copied; a failed upload
     // leaves the image to RunAlgorithm
     const bool up = I.can_upload() && I.ref.ensure(bytes) == MVS_OK;
+    if (up && mvs::page_locked(img, bytes)) {
+        if (mvs::direct_upload(I.ref.p, img, bytes, {{ps->ps.HostRef.data(), img, bytes}}, I.uploaded[0])) {
+            I.ref_dev = true;
+            I.dev_w = w;
+            I.dev_h = h;
+        }
+        return MVS_OK;
+    }
     const int rc = mvs::parallel_copy({{ps->ps.HostRef.data(), img, bytes, up ? I.ref.p : nullptr}}, 0);
     if (up && rc == 0 && cudaEventRecord(I.uploaded[0], 0) == cudaSuccess) {
         I.ref_dev = true;
@@ -773,13 +813,22 @@ int mvs_ps_set_sources(mvs_planesweep *ps, const float *imgs, int32_t n, const f
     I.srcs_dev = 0;
     const bool up = I.can_upload() && n > 0 && I.srcs.ensure(bytes * n) == MVS_OK;
     ps->ps.HostSrc.resize(n);
+    const bool direct = up && mvs::page_locked(imgs, bytes * n);
     std::vector<mvs::CopyPiece> pieces;
     for (int v = 0; v < n; ++v) {
         ps->ps.HostSrc[v].reset(w, h);
         pieces.push_back({ps->ps.HostSrc[v].data(), imgs + (size_t)v * w * h, bytes,
-                          up ? (void *)(I.srcs.as<char>() + bytes * v) : nullptr});
+                          up && !direct ? (void *)(I.srcs.as<char>() + bytes * v) : nullptr});
         ps->ps.HostSrc[v].R = Matrix3D(R9s + 9 * v);
         ps->ps.HostSrc[v].t = Vector3D(t3s + 3 * v);
+    }
+    if (direct) {
+        if (mvs::direct_upload(I.srcs.p, imgs, bytes * n, pieces, I.uploaded[1])) {
+            I.srcs_dev = n;
+            I.dev_w = w;
+            I.dev_h = h;
+        }
+        return MVS_OK;
     }
     const int rc = mvs::parallel_copy(pieces, 0);
     if (up && rc == 0 && cudaEventRecord(I.uploaded[1], 0) == cudaSuccess) {

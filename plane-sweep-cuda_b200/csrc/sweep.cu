@@ -421,7 +421,7 @@ constexpr int kFloorMagicBits = 0x4B400000;
 // the source's 2x2 neighbourhoods (difference form in COMPENSATED), else the
 // four samples are gathered from `src`.  COMPENSATED stores the samples
 // shifted by `shift`.
-template <int WIN, int MOM, bool QUAD, int TWS = 0>
+template <int WIN, int MOM, bool QUAD, int TWS = 0, bool ROWS_INTERIOR = false>
 __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__restrict__ src,
                                              const float4 *__restrict__ quad, int w, int h, const float *Hm, float X,
                                              const float *Yc, float shift)
@@ -449,7 +449,8 @@ __device__ __forceinline__ void pass_a0_rows(float (*Wt)[RWMAX], const float *__
             fa[j] = fb[j] = 0.f;
             off[j] = 0u;
             if (k < CELLS && rb + 3 * k < G::RH) {
-                const float Y = Yc[rb + 3 * k];
+                // ROWS_INTERIOR: no region row is mirrored, so the rows are consecutive
+                const float Y = ROWS_INTERIOR ? Yc[rb] + (float)(3 * k) : Yc[rb + 3 * k];
                 float xs, ys;
                 if (MOM == MVS_MOMENTS_REFERENCE) {
                     const float q0 = Hm[0] * X + Hm[1] * Y + Hm[2] * 1.f;
@@ -584,11 +585,15 @@ __device__ __forceinline__ void pass_a1_rows(const float (*Wt)[RWMAX], float (*C
 }
 
 // One CTA's work: tile (tx, ty) of the frame, planes of `chunk`.
-// HWCVT: round the costs to BF16 with the hardware conversion (the same bits
-// as f2bf); the batched kernel, whose seven inlined window bodies share one
-// register allocation, rounds them with f2bf, which ptxas spills less around
-// (59.2 against 61.7 ms on the bench's batch of 48 frames).
-template <int WIN, int MOM, int TWS = 0, bool HWCVT = true>
+// BATCHED: the batched kernel's instantiation, whose seven inlined window
+// bodies share one register allocation.  Two choices differ there, each
+// measured on the bench's batch of 48 frames: the costs are rounded to BF16
+// by f2bf instead of the hardware conversion (the same bits; ptxas spills
+// less around it: 59.2 against 61.7 ms), and tiles whose region rows are all
+// inside the frame form the row coordinates instead of reading them (58.5
+// against 59.1 ms; in the single-frame kernel that form issued 2% more
+// instructions and was slower).
+template <int WIN, int MOM, int TWS = 0, bool BATCHED = false>
 __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, int tx, int ty, int chunk)
 {
     using G = Geo<WIN, TWS>;
@@ -608,6 +613,9 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
     }
     ref_moments<WIN, MOM, TWS>(S.Wt, S.CS, shift, a.stdthresh, A.RM, A.RS);
     const float Xcol = (float)(mirror_idx(x0 - G::R + (int)(threadIdx.x % G::RW), w) + 1);
+    // every region row inside the frame: pass A0 forms the row coordinates
+    // instead of reading them (batched kernel only)
+    const bool rows_interior = BATCHED && y0 - G::R >= 0 && y0 - G::R + G::RH <= h;
 
     const int ly = b_row(), lx = b_seg() * G::RUN;
     const int y = y0 + ly, xb = x0 + lx;
@@ -639,7 +647,10 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             const int nv = last_view ? 0 : view + 1, np = last_view ? p + 1 : p;
             float hn = 0.f;
             if (threadIdx.x < 9 && np < p1) hn = ldg(a.H + ((size_t)nv * a.P + np) * 9 + threadIdx.x);
-            if (a.quad)
+            if (a.quad && rows_interior)
+                pass_a0_rows<WIN, MOM, true, TWS, true>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc,
+                                                        sh);
+            else if (a.quad)
                 pass_a0_rows<WIN, MOM, true, TWS>(S.Wt, nullptr, a.quad + (size_t)view * n, w, h, Hm, Xcol, A.Yc, sh);
             else
                 pass_a0_rows<WIN, MOM, false, TWS>(S.Wt, a.srcs + (size_t)view * n, nullptr, w, h, Hm, Xcol, A.Yc, sh);
@@ -662,7 +673,7 @@ __device__ __forceinline__ void aggregated_tile(AggSmem &A, const SweepArgs &a, 
             // below 0; the stored bf16 bits then order like unsigned integers)
             float cf = fmaf(-acc[j], invV, 1.f);
             cf = cf > 0.f ? cf : (cf == cf ? 0.f : 3.f);
-            cb[j] = HWCVT ? f2bf_num(cf) : f2bf(cf);   // cf is not NaN here
+            cb[j] = BATCHED ? f2bf(cf) : f2bf_num(cf);   // cf is not NaN here
             best[j] = min(best[j], ((uint32_t)cb[j] << 16) | (uint32_t)p);
         }
         if (a.cost && y < h) {
@@ -1286,13 +1297,13 @@ __global__ void __launch_bounds__(THREADS, 3) sweep_batch_kernel(const BatchFram
         a.quad = f.quad;
         const int tx = (int)item.y % f.tiles_x, ty = (int)item.y / f.tiles_x;
         switch (f.win) {
-        case 3: aggregated_tile<3, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        case 5: aggregated_tile<5, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        case 7: aggregated_tile<7, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        case 9: aggregated_tile<9, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        case 11: aggregated_tile<11, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        case 13: aggregated_tile<13, MOM, TWS, false>(S, a, tx, ty, item.z); break;
-        default: aggregated_tile<15, MOM, TWS, false>(S, a, tx, ty, item.z); break;
+        case 3: aggregated_tile<3, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        case 5: aggregated_tile<5, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        case 7: aggregated_tile<7, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        case 9: aggregated_tile<9, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        case 11: aggregated_tile<11, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        case 13: aggregated_tile<13, MOM, TWS, true>(S, a, tx, ty, item.z); break;
+        default: aggregated_tile<15, MOM, TWS, true>(S, a, tx, ty, item.z); break;
         }
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -129,6 +129,40 @@ def test_images_set_again_between_runs(cuda, golden):
         p.close()
 
 
+def test_page_locked_images_are_uploaded_from_the_callers_memory(cuda, golden):
+    """Images in page-locked memory are uploaded from the caller's buffer while the handle
+    copies them: the depthmaps equal the reference's, and the caller may overwrite its buffers
+    as soon as the setter returns (the run still sees the images it was given)."""
+    import torch
+    g = golden("sweep_inverse_w5")
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()
+        return t, t.numpy()
+
+    t_ref, h_ref = pinned(g["ref"])
+    t_srcs, h_srcs = pinned(np.asarray(g["srcs"]))
+    ps = make_ps(g, True)
+    ps.set_reference(h_ref, g["Rref"], g["tref"])
+    ps.set_sources(h_srcs, np.asarray(g["Rsrc"]), np.asarray(g["tsrc"]))
+    h_ref[...] = 0.0
+    h_srcs[...] = 0.0
+    ps.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), g["depth"])
+    # other sources through the same pinned buffer, against a fresh handle fed pageable arrays
+    g2 = dict(g)
+    g2["srcs"], g2["Rsrc"], g2["tsrc"] = g["srcs"][::-1], g["Rsrc"][::-1], g["tsrc"][::-1]
+    h_srcs[...] = np.asarray(g2["srcs"])
+    ps.set_sources(h_srcs, np.asarray(g2["Rsrc"]), np.asarray(g2["tsrc"]))
+    h_srcs[...] = 0.0
+    ps.RunAlgorithm()
+    fresh = make_ps(g2, True)
+    fresh.RunAlgorithm()
+    np.testing.assert_array_equal(ps.getDepthmap(), fresh.getDepthmap())
+    for p in (ps, fresh):
+        p.close()
+
+
 def test_getters_refuse_a_map_of_another_frame_size(cuda, golden):
     """After the reference is set again at another size, the last run's maps no
     longer fit the getters' width*height contract: they are refused, not copied."""
