@@ -307,9 +307,11 @@ int mvs_ps_destroy(mvs_planesweep *ps);
 /* HostRef / HostSrc with their R, t (planesweep.h:31-34, cam_image.h:10-11).
  * The images are copied into the handle's page-locked host images and
  * uploaded to the device in the same pass (on the default stream, MB by MB as
- * they are copied); RunAlgorithm then uploads neither.  The caller's buffers
- * are free again when the call returns.  Without a device the images stay on
- * the host. */
+ * they are copied); RunAlgorithm then uploads neither.  Images in page-locked
+ * memory (mvs_host_alloc, cudaHostAlloc, registered) are uploaded in one copy
+ * from the caller's buffer while they are copied, which the link runs faster.
+ * Either way the caller's buffers are free again when the call returns.
+ * Without a device the images stay on the host. */
 int mvs_ps_set_reference(mvs_planesweep *ps, const float *h_img, int32_t width, int32_t height, const float *R9,
                          const float *t3);
 int mvs_ps_set_sources(mvs_planesweep *ps, const float *h_imgs, int32_t n, const float *R9s, const float *t3s);
