@@ -110,9 +110,17 @@ __global__ void __launch_bounds__(VX *VY) histogram_kernel(Dims D, uint16_t *__r
         const float k2 = ldg(K + 6) * r0 + ldg(K + 7) * r1 + ldg(K + 8) * r2;
         const float px = k0 / k2, py = k1 / k2;
         if ((px < 0) || (px > w - 1) || (py < 0) || (py > h - 1)) continue;
-        const float flx = floorf(px), fly = floorf(py);
-        const int x0 = (int)fmaxf(flx, 0), y0 = (int)fmaxf(fly, 0);
-        const int x1 = (int)fminf(x0 + 1, w - 1), y1 = (int)fminf(y0 + 1, h - 1);
+        // The reference's floorf, (int)fmaxf(., 0) and (int)fminf(x0 + 1, w - 1),
+        // without the conversion unit: here 0 <= p <= w - 1 < 2^22 (or p is
+        // NaN, which fmaxf turns into 0 as the reference's does, and the
+        // fraction stays NaN), so p + 1.5 * 2^23 rounded down is 1.5 * 2^23 +
+        // floor(p) exactly, whose low bits are floor(p) (a standard
+        // magic-number floor).
+        const float pxc = fmaxf(px, 0.f), pyc = fmaxf(py, 0.f);
+        const float tx = __fadd_rd(pxc, 12582912.f), ty = __fadd_rd(pyc, 12582912.f);
+        const float flx = tx - 12582912.f, fly = ty - 12582912.f;
+        const int x0 = __float_as_int(tx) - 0x4B400000, y0 = __float_as_int(ty) - 0x4B400000;
+        const int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
         const float frx = px - flx, fry = py - fly;
         const float *dm = depths + (size_t)m * w * h;
         const float d00 = ldg(dm + x0 + y0 * w), d10 = ldg(dm + x1 + y0 * w);
@@ -159,12 +167,16 @@ __device__ __forceinline__ float prox_median(const uint32_t *cnt, float u, float
 #pragma unroll
     for (int k = 0; k < BINS; ++k) total += (int)cnt[k];
     float Bv[BINS];   // ascending
+    // (float)W without the conversion unit: |W| <= total < 2^22, so the bits
+    // 0x4B400000 + W are the float 1.5 * 2^23 + W exactly, and subtracting
+    // 1.5 * 2^23 leaves W exactly (a standard magic-number conversion)
+    const int biased = total + 0x4B400000;
     int pre = 0;
 #pragma unroll
     for (int j = 1; j <= BINS; ++j) {
         pre += (int)cnt[j - 1];
-        const int W = total - 2 * pre;   // Wi(j), fusion.h:813-820
-        const float pj = u + tl * (float)W;
+        const float W = __int_as_float(biased - 2 * pre) - 12582912.f;   // Wi(j), fusion.h:813-820
+        const float pj = u + tl * W;
         Bv[BINS - j] = fmaxf(pj, -1.f);
     }
     const float NEG = -INFINITY, POS = INFINITY;
