@@ -154,14 +154,16 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
 {
     using S = ConvSmem<COUT>;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = (uint64_t *)(smem + 2 * S::STAGE);
-    uint32_t *tmem_slot = (uint32_t *)(smem + 2 * S::STAGE + 16);
+    const int H = a.H, W = a.W, cin = a.cin;
+    const int nslices = cin >> 4;
+    // one 16-channel slice needs one stage (launch_conv_t gives the CTA that much)
+    const int nstages = nslices > 1 ? 2 : 1;
+    uint64_t *bars = (uint64_t *)(smem + nstages * S::STAGE);
+    uint32_t *tmem_slot = (uint32_t *)(smem + nstages * S::STAGE + 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int b = blockIdx.y;
     const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
     const int x0 = tx * TW, y0 = ty * TH;
-    const int H = a.H, W = a.W, cin = a.cin;
-    const int nslices = cin >> 4;
     const size_t img = (size_t)H * W;
 
     if (warp == 0) tmem_alloc(tmem_slot, S::TMEM_COLS);
@@ -296,7 +298,9 @@ int launch_conv_t(const ConvArgs &a, int B, cudaStream_t st)
     using S = ConvSmem<COUT>;
     MVS_TRY_CUDA(cudaFuncSetAttribute(conv3x3_tc_kernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
     const int tiles = a.tiles_x * ceil_div(a.H, TH);
-    conv3x3_tc_kernel<COUT><<<dim3(tiles, B), CONV_THREADS, S::BYTES, st>>>(a);
+    // a 16-channel input is one slice: one stage, so more CTAs share an SM
+    const int bytes = a.cin > 16 ? S::BYTES : S::STAGE + 64;
+    conv3x3_tc_kernel<COUT><<<dim3(tiles, B), CONV_THREADS, bytes, st>>>(a);
     return MVS_OK;
 }
 
