@@ -41,6 +41,8 @@ constexpr int HW_ = TW + 2, HH_ = TH + 2;     // halo
 constexpr int HALO_PIX = HW_ * HH_;           // 180
 constexpr int HALO_BYTES = 2 * HALO_PIX * 16; // two 8-channel planes
 constexpr int CONV_THREADS = 128;
+// output tiles per CTA of the convolution at 16 and 32 output channels
+constexpr int CONV_MT16 = 2, CONV_MT32 = 2;
 
 // ---------------------------------------------------------------------------
 // tcgen05 / mbarrier helpers (inline PTX, sm_100a)
@@ -141,18 +143,24 @@ constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s
         if (rc__) return rc__;    \
     } while (0)
 
-template <int COUT>
+// MT output tiles of 8 x 16 pixels stacked vertically per CTA: they share
+// one (MT * 16 + 2)-row halo and one copy of the weights, and accumulate in
+// MT column blocks of COUT in tensor memory.
+template <int COUT, int MT = 1>
 struct ConvSmem {
+    static constexpr int HALO_ROWS = MT * TH + 2;
+    static constexpr int HPIX = HW_ * HALO_ROWS;          // halo pixels
+    static constexpr int HBYTES = 2 * HPIX * 16;          // two 8-channel planes
     static constexpr int W_BYTES = 9 * 2 * COUT * 16;
-    static constexpr int STAGE = HALO_BYTES + W_BYTES;
+    static constexpr int STAGE = (HBYTES + W_BYTES + 127) / 128 * 128;
     static constexpr int BYTES = 2 * STAGE + 64;
-    static constexpr int TMEM_COLS = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;
+    static constexpr int TMEM_COLS = MT * COUT <= 32 ? 32 : MT * COUT <= 64 ? 64 : MT * COUT <= 128 ? 128 : 256;
 };
 
-template <int COUT>
+template <int COUT, int MT = 1>
 __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
 {
-    using S = ConvSmem<COUT>;
+    using S = ConvSmem<COUT, MT>;
     extern __shared__ __align__(128) unsigned char smem[];
     const int H = a.H, W = a.W, cin = a.cin;
     const int nslices = cin >> 4;
@@ -163,7 +171,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int b = blockIdx.y;
     const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
-    const int x0 = tx * TW, y0 = ty * TH;
+    const int x0 = tx * TW, y0 = ty * (MT * TH);
     const size_t img = (size_t)H * W;
 
     if (warp == 0) tmem_alloc(tmem_slot, S::TMEM_COLS);
@@ -180,14 +188,14 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
 
     // stage slice c into buffer s: halo pixels (2 x 16 B) and 9 taps of weights
     auto load = [&](int c, int s) {
-        const uint32_t hb = sbase + s * S::STAGE, wb = hb + HALO_BYTES;
-        for (int k = tid; k < 2 * HALO_PIX; k += CONV_THREADS) {
+        const uint32_t hb = sbase + s * S::STAGE, wb = hb + S::HBYTES;
+        for (int k = tid; k < 2 * S::HPIX; k += CONV_THREADS) {
             const int pix = k >> 1, half = k & 1;
             const int hy = pix / HW_, hx = pix - hy * HW_;
             const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
             const bool ok = gy >= 0 && gy < H && gx >= 0 && gx < W;
             const bf16 *src = a.in + ((size_t)b * img + (ok ? (size_t)gy * W + gx : 0)) * cin + 16 * c + 8 * half;
-            cp_async16(hb + (half * HALO_PIX + pix) * 16, src, ok);
+            cp_async16(hb + (half * S::HPIX + pix) * 16, src, ok);
         }
         constexpr int WV = 2 * COUT;   // 16-byte vectors per tap
         for (int k = tid; k < 9 * WV; k += CONV_THREADS) {
@@ -207,13 +215,16 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
         const int s = c & 1;
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t hb = sbase + s * S::STAGE, wb = hb + HALO_BYTES;
+            const uint32_t hb = sbase + s * S::STAGE, wb = hb + S::HBYTES;
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
                 const int ky = t / 3, kx = t - 3 * ky;
-                const uint64_t ad = smem_desc(hb + (ky * HW_ + kx) * 16, HALO_PIX * 16, HW_ * 16);
                 const uint64_t bd = smem_desc(wb + t * 2 * COUT * 16, COUT * 16, 128);
-                mma_bf16(tmem, ad, bd, idesc, (c > 0 || t > 0) ? 1u : 0u);
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt) {
+                    const uint64_t ad = smem_desc(hb + ((mt * TH + ky) * HW_ + kx) * 16, S::HPIX * 16, HW_ * 16);
+                    mma_bf16(tmem + (uint32_t)(mt * COUT), ad, bd, idesc, (c > 0 || t > 0) ? 1u : 0u);
+                }
             }
             mma_commit(&bars[s]);
         }
@@ -249,15 +260,17 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
     }
     tc_fence_after();
 
-    // epilogue: thread = accumulator row = pixel
+    // epilogue: thread = accumulator row = pixel (of each of the MT tiles)
     const int m = warp * 32 + lane;
-    const int py = y0 + (m >> 3), px = x0 + (m & 7);
+#pragma unroll 1
+    for (int mt = 0; mt < MT; ++mt) {
+    const int py = y0 + mt * TH + (m >> 3), px = x0 + (m & 7);
     const bool inside = py < H && px < W;
     const size_t pidx = (size_t)b * img + (size_t)min(py, H - 1) * W + min(px, W - 1);
 #pragma unroll 1
     for (int c0 = 0; c0 < COUT; c0 += 16) {
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * COUT + c0), v);
         if (a.bias) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) v[k] += a.bias[c0 + k];
@@ -284,6 +297,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
                                pack_bf16x2(v[14], v[15]));
         }
     }
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -292,15 +306,16 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3x3_tc_kernel(ConvArgs a)
     }
 }
 
-template <int COUT>
+template <int COUT, int MT = 1>
 int launch_conv_t(const ConvArgs &a, int B, cudaStream_t st)
 {
-    using S = ConvSmem<COUT>;
-    MVS_TRY_CUDA(cudaFuncSetAttribute(conv3x3_tc_kernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
-    const int tiles = a.tiles_x * ceil_div(a.H, TH);
+    using S = ConvSmem<COUT, MT>;
+    MVS_TRY_CUDA(cudaFuncSetAttribute(conv3x3_tc_kernel<COUT, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      S::BYTES));
+    const int tiles = a.tiles_x * ceil_div(a.H, MT * TH);
     // a 16-channel input is one slice: one stage, so more CTAs share an SM
     const int bytes = a.cin > 16 ? S::BYTES : S::STAGE + 64;
-    conv3x3_tc_kernel<COUT><<<dim3(tiles, B), CONV_THREADS, bytes, st>>>(a);
+    conv3x3_tc_kernel<COUT, MT><<<dim3(tiles, B), CONV_THREADS, bytes, st>>>(a);
     return MVS_OK;
 }
 
@@ -310,8 +325,8 @@ int launch_conv(const bf16 *in, int cin, const bf16 *wpack, const float *bias, c
     if (cin <= 0 || cin % 16 || cin > 512) return set_error(MVS_ERR_ARG, "conv input channels %d (multiple of 16)", cin);
     ConvArgs a{in, wpack, bias, mask, out, err, H, W, cin, relu, ceil_div(W, TW)};
     switch (cout) {
-    case 16: return launch_conv_t<16>(a, B, st);
-    case 32: return launch_conv_t<32>(a, B, st);
+    case 16: return launch_conv_t<16, CONV_MT16>(a, B, st);
+    case 32: return launch_conv_t<32, CONV_MT32>(a, B, st);
     case 48: return launch_conv_t<48>(a, B, st);
     case 64: return launch_conv_t<64>(a, B, st);
     case 96: return launch_conv_t<96>(a, B, st);
