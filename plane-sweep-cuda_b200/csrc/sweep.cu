@@ -42,6 +42,7 @@
 #include <string.h>
 
 #include "common.cuh"
+#include "div_win.cuh"
 
 namespace mvs {
 namespace {
@@ -108,24 +109,6 @@ struct SweepArgs {
 // the REFERENCE path keeps the reference's dot-product order).  Cells are processed in
 // batches -- coordinates, then all gathers, then the interpolation -- so each
 // thread keeps several independent L1/L2 gathers in flight.
-
-// x / WIN rounded to nearest, as the reference divides its window sums by the
-// window side, in three instructions instead of a division: with
-// y = RN(1 / WIN), q = RN(x y) is within one ulp of x / WIN, the residual
-// x - q WIN is exact in one fused multiply-add, and RN(q + residual * y) is
-// the correctly rounded quotient (Markstein's correction: P. W. Markstein,
-// IBM J. Res. Dev. 34(1), 1990).  Zero, infinite and NaN x keep q, which is
-// then exact (the correction would turn -0 into +0 and inf into NaN).
-// Compared with the IEEE division for every float bit pattern and every
-// window side 3..15 on a B200: no difference.
-template <int WIN>
-__device__ __forceinline__ float div_win(float x)
-{
-    constexpr float d = (float)WIN, y = 1.f / (float)WIN;
-    const float q = __fmul_rn(x, y);
-    const float r = __fmaf_rn(-q, d, x);
-    return isfinite(x) && x != 0.f ? __fmaf_rn(r, y, q) : q;
-}
 
 // ---- pass B: row sums of one column-sum array --------------------------------------
 
